@@ -1,0 +1,325 @@
+"""Benchmark of the leap-frog path: DOF-steps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the 64-shot batched configuration -- 200x100 jittered
+squares (40,000 triangles), Dubiner N=5 (1.68 M DOFs per shot), per-element
+log-normal vp, 64 Ricker shots at seeded interior points, 128 surface
+receivers, dt = 0.4 x CFL from a device power iteration -- with FP32 operator
+blocks, FP32 accumulation and FP64 state. One bench "step" is one leap-frog
+step of all 64 shots. Under torchrun each rank runs its own 64 shots (weak
+scaling, no collective in the data path); the timed region is bracketed by a
+barrier and a device synchronise, timed with CUDA events on the engine's
+stream, max over ranks.
+
+Also reported: the plain FP64 single-shot drop-in on the same mesh, the
+seismogram error of the measured form against FP64 over the full step count,
+an end-to-end number through the public C-ABI with host buffers, the
+roofline of the step kernel and the reference's CPU path on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from tspeed_b200 import capi  # noqa: E402
+from tspeed_b200 import workloads as W  # noqa: E402
+
+METRIC = "DOF-steps/s on 1 B200: mixed/batched vs plain FP64, at seismogram err <=1e-4"
+UNIT = "DOF-steps/s"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "tsp_ref_run")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_per_step(ne, Np, nnzb, nshots, precision):
+    """Algorithmic HBM bytes of one step: every block once, the state read
+    (u^k, u^{k-1}) and written (u^{k+1}) once per shot, minv once."""
+    R = 2 * Np
+    bblk = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
+    extra = nnzb * 4 if precision == "bf16" else 0
+    return nnzb * R * R * bblk + extra + nshots * 2 * ne * Np * 24 + ne * 8
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        self.index = vis.split(",")[local_rank].strip() if vis else str(local_rank)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_problem(args, rank):
+    p = W.config(3, scale=args.scale, nshots=args.nshots, shot_seed=1000 + rank)
+    return p
+
+
+def estimate_dt(sim, cfl_fraction=0.4, iters=60):
+    lmax = sim.estimate_lmax(iters)
+    return cfl_fraction * 2.0 / math.sqrt(lmax), lmax
+
+
+def prepare(sim, prob, dt, nsteps):
+    sim.set_dt(dt)
+    for k, s in enumerate(prob.sources):
+        sim.set_ricker(k, s.f0, s.t0, s.amp, s.direction, nsteps)
+
+
+def cpu_reference_sample(nprocs=1, nsteps=300, scale=0.2, timeout=600):
+    """The reference's own CPU path (oracle/_ref, compiled from its sources)
+    on a bounded sample of the workload: the same configuration shrunk to
+    `scale` per axis, one shot per process, `nprocs` processes in parallel
+    (the reference is single-threaded). Returns (DOF-steps/s, sample text)."""
+    if not os.path.exists(REF_BIN):
+        return None, "reference binary missing"
+    p = W.config(3, scale=scale, nshots=max(1, nprocs))
+    ne, Np = p.mesh.ne, p.Np
+    with tempfile.TemporaryDirectory() as tmp:
+        msh, rcv, mat = (os.path.join(tmp, n) for n in ("m.msh", "m.rcv", "m.mat"))
+        W.write_gmsh(msh, p.mesh)
+        W.write_rcv(rcv, p.receivers)
+        np.stack([p.lam, p.mu, p.rho], 1).astype(np.float64).tofile(mat)
+        procs = []
+        for k in range(nprocs):
+            s = p.sources[k]
+            cmd = [REF_BIN, "--mesh", msh, "--N", str(p.N), "--mat", mat, "--rcv", rcv, "--out",
+                   os.path.join(tmp, f"o{k}"), "--dt", "1e-4", "--nsteps", str(nsteps), "--src", repr(s.x),
+                   repr(s.y), "--ricker", repr(s.f0), repr(s.t0), repr(s.amp), "--penalty", repr(p.penalty)]
+            procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        loops = []
+        for pr in procs:
+            out, err = pr.communicate(timeout=timeout)
+            if pr.returncode != 0:
+                return None, "reference run failed: " + err.strip()[-200:]
+            loops.append(json.loads(out.strip().splitlines()[-1])["loop_s"])
+    dofs = 2 * ne * Np
+    value = nprocs * dofs * nsteps / max(loops)
+    sample = (f"{p.mesh.ne} triangles (config shrunk x{scale} per axis), N={p.N}, {nsteps} steps, "
+              f"{nprocs} single-threaded process(es), one shot each; loop time only")
+    return value, sample
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ncores = os.cpu_count() or 1
+    nsteps = max(10, args.steps)
+    v, sample = cpu_reference_sample(nprocs=ncores, nsteps=nsteps)
+    cfg = config_dict(args, None)
+    if v is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return 0
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def config_dict(args, prob):
+    d = {"workload": "64-shot batched DG leap-frog: 200x100 jittered squares (40,000 triangles), Dubiner N=5, "
+                     "log-normal vp, 128 receivers, FP32 blocks / FP64 state",
+         "mesh_triangles": prob.mesh.ne if prob else 40000, "N": 5, "shots_per_gpu": args.nshots,
+         "precision": args.precision, "dofs_per_shot": prob.dofs_per_shot if prob else 1680000,
+         "l2": "inputs larger than L2 (state 0.86 GB per level, blocks 1.1 GB)", "parallelism": f"shots x{args.gpus}"}
+    return d
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--nshots", type=int, default=64)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
+    ap.add_argument("--no-extras", action="store_true", help="skip plain-FP64, accuracy, e2e and CPU legs")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local_rank))
+        dist = tdist
+
+    prob = make_problem(args, rank)
+    K, Wm = args.steps, max(3, args.warmup)
+    sim = capi.Simulation.from_problem(prob, precision=args.precision, device=local_rank)
+    dt, lmax = estimate_dt(sim)
+    prepare(sim, prob, dt, K + Wm + 2)
+    sim.set_seismogram_capacity(K + Wm + 2)
+    sim.first_step()
+    sim.run(Wm)
+    sim.run_timed(K)  # instantiate the K-step graph outside the timed region
+    sampler = ClockSampler(local_rank)
+    if dist:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.4)
+    ms = sim.run_timed(K)
+    clocks = sampler.stop()
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    dofs = prob.dofs_per_shot
+    value = world * prob.nshots * dofs * K / (ms / 1e3)
+    ms_step = ms / K
+    hbm, peak_kind = peaks()
+    algo = bytes_per_step(prob.mesh.ne, prob.Np, sim.nnzb, prob.nshots, args.precision)
+    achieved = algo / (ms_step / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
+            "config": config_dict(args, prob), "dt": dt, "lmax": lmax,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_step": algo},
+            "gpu_launches": K + 1, "clocks": clocks}
+    sim.close()
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        # Plain FP64 single-shot drop-in on the same mesh.
+        p1 = W.config(3, scale=args.scale, nshots=1, shot_seed=1000)
+        with capi.Simulation.from_problem(p1, precision="fp64") as s1:
+            prepare(s1, p1, dt, K + Wm + 2)
+            s1.first_step()
+            s1.run(Wm)
+            s1.run_timed(K)
+            ms1 = s1.run_timed(K)
+            nnzb1 = s1.nnzb
+        v1 = p1.dofs_per_shot * K / (ms1 / 1e3)
+        a1 = bytes_per_step(p1.mesh.ne, p1.Np, nnzb1, 1, "fp64") / (ms1 / K / 1e3) / 1e9
+        line["plain_fp64_single_shot"] = {"value": v1, "unit": UNIT, "ms_per_step": ms1 / K,
+                                          "roofline_frac": a1 / hbm, "achieved_gbs": a1}
+        line["speedup_vs_plain_fp64"] = value / v1
+        # Accuracy of the measured form against FP64 over the full step count.
+        nacc = prob.nsteps if args.accuracy_steps < 0 else args.accuracy_steps
+        if args.precision != "fp64" and nacc > 0:
+            seis = {}
+            for prec in ("fp64", args.precision):
+                with capi.Simulation.from_problem(prob, precision=prec) as s:
+                    prepare(s, prob, dt, nacc)
+                    s.set_seismogram_capacity(nacc)
+                    s.first_step()
+                    s.run(nacc - 1)
+                    seis[prec] = s.seismograms(0, nacc)
+            ref = seis["fp64"]
+            err = float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))
+            line["seismogram_rel_l2_err_vs_fp64"] = err
+            line["accuracy_steps"] = nacc
+        # End to end through the public C-ABI with host buffers.
+        ne_steps = K
+        t0 = time.perf_counter()
+        with capi.Simulation.from_problem(prob, precision=args.precision) as s:
+            prepare(s, prob, dt, ne_steps)
+            s.set_seismogram_capacity(ne_steps)
+            s.first_step()
+            s.run(ne_steps - 1)
+            sg = s.seismograms(0, ne_steps)
+            us = [s.u(k) for k in range(prob.nshots)]
+        t_e2e = time.perf_counter() - t0
+        h2d = (prob.mesh.xy.nbytes + prob.mesh.tri.nbytes + 3 * prob.mesh.ne * 8 + prob.nshots * 16 +
+               len(prob.receivers) * 16 + prob.nshots * ne_steps * 16)
+        d2h = sg.nbytes + sum(u.nbytes for u in us)
+        line["e2e"] = {"value": prob.nshots * dofs * ne_steps / t_e2e, "unit": UNIT,
+                       "h2d_bytes_per_step": h2d / ne_steps, "d2h_bytes_per_step": d2h / ne_steps,
+                       "wall_s": t_e2e, "steps": ne_steps,
+                       "includes": "tsp_create (mesh upload, device assembly, point location), force tables, "
+                                   "first_step + run, seismogram and final-state read-back"}
+        v_cpu, sample = cpu_reference_sample(nprocs=1, nsteps=200)
+        line["cpu_baseline"] = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,235 @@
+/*
+ * tspeed_b200 C-ABI: B200 (sm_100a) engine for tspeed's explicit leap-frog
+ * time loop.
+ *
+ * The reference (carlomr/tspeed) exposes this path only as the header-only
+ * C++ class LeapFrog : TimeAdvance (lib/include/TimeAdvance.hpp:123-256),
+ * built from a Mesh, an FESpace<N>, Parameters, Receivers and a Force. This
+ * library is the thin, exception-free, plain-pointer boundary under a C++
+ * class of the same surface (include/tspeed_gpu.hpp). Each entry point below
+ * names the reference member it replaces.
+ *
+ * Conventions
+ *   - Every function returns an int status (tsp_status); 0 is success. Errors
+ *     never exit the process (the reference calls exit(), e.g. Mesh.cpp:184,
+ *     MyMat.cpp:40, Receivers_imp.hpp:50); the message of the last failure is
+ *     available from tsp_last_error().
+ *   - Host arrays are caller-owned and copied at call time. Device memory is
+ *     library-owned. One handle = one CUDA stream on one device; a handle is
+ *     not thread-safe (the reference is single-threaded).
+ *   - Displacement vectors on the host use the reference's layout
+ *     u[c*ne*Np + e*Np + i] (component c in {0,1}, element e, mode i;
+ *     FESpace_imp.hpp:152-153). On the device the library keeps an
+ *     element-major, shot-interleaved layout.
+ *   - tsp_first_step, tsp_step and tsp_run allocate no device memory;
+ *     tsp_run instantiates a CUDA graph the first time it sees a step count
+ *     (per parity of the current level) and replays it afterwards.
+ */
+#ifndef TSPEED_B200_H
+#define TSPEED_B200_H 1
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSP_ABI_VERSION 1
+
+typedef struct tsp_handle tsp_handle;
+
+typedef enum {
+  TSP_OK = 0,
+  TSP_ERR_ARG = -1,         /* invalid argument */
+  TSP_ERR_CUDA = -2,        /* CUDA runtime error */
+  TSP_ERR_NOMEM = -3,       /* device or host allocation failed */
+  TSP_ERR_STATE = -4,       /* call out of order (e.g. step before first_step) */
+  TSP_ERR_NOT_FOUND = -5,   /* source/receiver point outside the mesh */
+  TSP_ERR_MESH = -6,        /* malformed mesh (clockwise triangle, non-manifold edge, bad file) */
+  TSP_ERR_NONFINITE = -7,   /* NaN/Inf detected in the state */
+  TSP_ERR_TIMEOUT = -8,     /* a bounded device-side wait gave up */
+  TSP_ERR_UNSUPPORTED = -9  /* option not built for this degree/precision */
+} tsp_status;
+
+/* Storage of the operator blocks. The state, the recurrence, M^-1 and the
+ * receivers always stay in FP64. */
+typedef enum {
+  TSP_PREC_FP64 = 0,  /* plain drop-in: FP64 blocks, FP64 accumulation */
+  TSP_PREC_FP32 = 1,  /* FP32 blocks, FP32 accumulation */
+  TSP_PREC_BF16 = 2   /* BF16 blocks with one FP32 scale per block, FP32 accumulation */
+} tsp_precision;
+
+typedef enum {
+  TSP_OP_EXPLICIT = 0,    /* assembled 2Np x 2Np blocks in HBM */
+  TSP_OP_MATRIX_FREE = 1  /* blocks rebuilt on the fly from reference-element matrices */
+} tsp_operator_kind;
+
+/*
+ * A simulation set up as the reference does it: mesh (Mesh.hpp:47), degree N
+ * of FESpace<N> with the default Gauss<N+1> rule and Dubiner<N> basis
+ * (FESpace.hpp:37), per-element Lame parameters and density (Parameters,
+ * FESpace.hpp:194-247), one point source per shot (PointWiseForce,
+ * Force.hpp:56-86) and receivers shared by all shots (Receivers,
+ * Receivers.hpp:77-121). The operator B = penalty*N^2*S + I + A
+ * (TimeAdvance_imp.hpp:32) is assembled on the device.
+ */
+typedef struct {
+  int32_t nverts;
+  const double* xy;       /* [nverts][2] */
+  int32_t ne;
+  const int32_t* tri;     /* [ne][3] 0-based vertex ids, counter-clockwise */
+  int32_t N;              /* Dubiner degree, 1..8 */
+  const double* lambda;   /* [ne] */
+  const double* mu;       /* [ne] */
+  const double* rho;      /* [ne] */
+  double penalty;         /* c of the c*N^2*S penalty term (reference default 2) */
+  int32_t precision;      /* tsp_precision */
+  int32_t op_kind;        /* tsp_operator_kind */
+  int32_t nshots;         /* >= 1 */
+  const double* src_xy;   /* [nshots][2] source points */
+  int32_t nrcv;           /* >= 0 */
+  const double* rcv_xy;   /* [nrcv][2] receiver points */
+  int32_t device;         /* CUDA device ordinal */
+} tsp_problem;
+
+/*
+ * A simulation whose operator was assembled elsewhere (e.g. by the
+ * reference's Matrices, TimeAdvance.hpp:56-119): block-CSR pattern of MyMat
+ * (MyMat.cpp:128-154, diagonal block first), FP64 blocks in merged component
+ * layout blocks[b][m*Np+i][n*Np+j] = B^{mn}(row, col[b])_{ij}, and the
+ * inverse-mass scalars minv[e] = 1/(rho_e detJ_e) (Matrices_imp.hpp:187,189).
+ */
+typedef struct {
+  int32_t ne;
+  int32_t Np;
+  int32_t nnzb;
+  const int32_t* row_ptr;  /* [ne+1] */
+  const int32_t* col;      /* [nnzb] */
+  const double* blocks;    /* [nnzb][2Np][2Np] row-major */
+  const double* minv;      /* [ne] */
+  int32_t precision;       /* tsp_precision */
+  int32_t nshots;
+  const int32_t* src_elem; /* [nshots] */
+  const double* src_phi;   /* [nshots][Np] basis values at the source point */
+  int32_t nrcv;
+  const int32_t* rcv_elem; /* [nrcv] */
+  const double* rcv_phi;   /* [nrcv][Np] */
+  int32_t device;
+} tsp_block_problem;
+
+/* Library version and build information ("tspeed_b200 <ver> sm_100a"). */
+const char* tsp_version(void);
+
+/* Constructor: replaces LeapFrog(Xh, p, r) (TimeAdvance_imp.hpp:29-33) plus
+ * the Receivers / PointWiseForce constructors. Locates sources and receivers
+ * (first containing element, Receivers_imp.hpp:34-51) and assembles B. */
+int tsp_create(const tsp_problem* prob, tsp_handle** out);
+
+/* Constructor from an externally assembled operator. */
+int tsp_create_from_blocks(const tsp_block_problem* prob, tsp_handle** out);
+
+/* Releases every resource of the handle. NULL is accepted. */
+int tsp_destroy(tsp_handle* h);
+
+/* Message of the last failing call on this handle (or of the last failing
+ * create, when h is NULL). Never NULL. */
+const char* tsp_last_error(const tsp_handle* h);
+
+/* Problem sizes: ne, Np, nshots, nrcv, nnzb (NULL pointers are skipped). */
+int tsp_get_sizes(const tsp_handle* h, int32_t* ne, int32_t* Np, int32_t* nshots, int32_t* nrcv, int64_t* nnzb);
+
+/* TimeAdvance::set_dt (TimeAdvance.hpp:153). */
+int tsp_set_dt(tsp_handle* h, double dt);
+
+/* Force of one shot as a table over leap-frog steps: F[k] = (Fx, Fy) at the
+ * time step k evaluates (k = 0: first_step at t = 0, TimeAdvance.cpp:28;
+ * k >= 1: t = t_{k-1} + dt accumulated in double, TimeAdvance.cpp:46). Steps
+ * past n use a zero force. Replaces add_force (TimeAdvance.hpp:171) with a
+ * PointWiseForce of the given time function (Force.cpp:22-30). */
+int tsp_set_force_table(tsp_handle* h, int32_t shot, const double* F, int64_t n);
+
+/* Convenience: the same table for a Ricker wavelet
+ * F_dir(t) = amp*(1 - 2 pi^2 f0^2 (t-t0)^2) exp(-pi^2 f0^2 (t-t0)^2)
+ * (Examples/src/Lamb.cpp:37), direction 0 (x) or 1 (y), n steps. Requires dt. */
+int tsp_set_ricker(tsp_handle* h, int32_t shot, double f0, double t0, double amp, int32_t direction, int64_t n);
+
+/* Force evaluation times of steps 0..n-1 for a given dt (see above). */
+int tsp_force_times(double dt, int64_t n, double* out);
+
+/* set_initial_u / set_initial_v (TimeAdvance.hpp:179-188): modal
+ * coefficients of u0 and v0 for one shot, reference layout; NULL = zero.
+ * Resets the step counter. */
+int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double* v0);
+
+/* LeapFrog::first_step (TimeAdvance.cpp:24-39). */
+int tsp_first_step(tsp_handle* h);
+
+/* LeapFrog::step (TimeAdvance.cpp:41-59), once. */
+int tsp_step(tsp_handle* h);
+
+/* nsteps calls of LeapFrog::step, replayed from a cached CUDA graph. */
+int tsp_run(tsp_handle* h, int64_t nsteps);
+
+/* tsp_run with CUDA events recorded on the handle's stream around the graph
+ * replay; synchronises and returns the device time in milliseconds. */
+int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
+
+/* Number of leap-frog steps done (first_step counts as 1) and the
+ * reference's M_last_time. */
+int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time);
+
+/* TimeAdvance::u() (TimeAdvance.hpp:202-203) of one shot, reference layout,
+ * length 2*ne*Np. Synchronises the handle's stream. */
+int tsp_get_u(tsp_handle* h, int32_t shot, double* out);
+
+/* Receiver samples, taken after every step on the device (the arithmetic of
+ * TimeAdvance::eval_receivers, TimeAdvance.cpp:68-79): out[shot][k][r][2]
+ * for steps k in [k0, k0+nk). k = 0 is the sample after first_step. */
+int tsp_get_seismograms(tsp_handle* h, int64_t k0, int64_t nk, double* out);
+
+/* Capacity of the on-device seismogram buffer, in steps (default 4096);
+ * samples of later steps wrap around modulo the capacity. */
+int tsp_set_seismogram_capacity(tsp_handle* h, int64_t nsteps);
+
+/* Enables the discrete-energy monitor E^{k} = 1/2|u^{k}-u^{k-1}|_M^2/dt^2 +
+ * 1/2 (u^{k})^T B u^{k-1}, summed over shots, recorded per step in FP64. */
+int tsp_enable_energy(tsp_handle* h, int32_t on);
+int tsp_get_energy(tsp_handle* h, int64_t k0, int64_t nk, double* out);
+
+/* Checkpoint / resume: both leap-frog levels (u^{k-1}, u^{k}) of every
+ * shot, reference layout, [nshots][2*ne*Np] each, plus the step counter. */
+int tsp_get_state(tsp_handle* h, double* u_prev, double* u_cur, int64_t* steps_done, double* last_time);
+int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int64_t steps_done, double last_time);
+
+/* Sets *bad to 1 if any displacement value of the current level is not
+ * finite (NaN/Inf watchdog). */
+int tsp_check_finite(tsp_handle* h, int32_t* bad);
+
+/* One product y = B x with the handle's operator (MyMatMultiDim::vecMult,
+ * MyMat.hpp:311-319), reference layout, shot 0. */
+int tsp_apply(tsp_handle* h, const double* x, double* y);
+
+/* Largest eigenvalue of M^-1 B by power iteration on the device (the
+ * reference has no CFL estimate; dt is a user setting). dt_cfl = 2/sqrt(lmax). */
+int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax);
+
+/* Exports of the assembled operator (explicit FP64 handles only):
+ * row_ptr[ne+1], col[nnzb], blocks[nnzb][2Np][2Np] row-major, minv[ne]. */
+int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* blocks, double* minv);
+
+/* Source and receiver location: elements and basis values. */
+int tsp_export_points(tsp_handle* h, int32_t* src_elem, double* src_phi, int32_t* rcv_elem, double* rcv_phi);
+
+/* Host-side mesh services (Mesh.cpp). */
+/* Gmsh 2.2 ASCII reader (Mesh::Mesh, Mesh.cpp:174-257): counts first
+ * (xy/tri/region NULL), then data. region = elementary tag. */
+int tsp_gmsh_read(const char* path, int32_t* nverts, double* xy, int32_t* ne, int32_t* tri, int32_t* region);
+/* Neighbour tables (Mesh::M_neighbors, Mesh.cpp:33-128) in O(ne):
+ * neigh[ne][3] (-1 on the boundary), neighedge[ne][3]. */
+int tsp_mesh_neighbours(int32_t ne, const int32_t* tri, int32_t* neigh, int32_t* neighedge);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSPEED_B200_H */

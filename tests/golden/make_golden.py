@@ -1,0 +1,119 @@
+"""Generates the golden fixtures in this folder from the reference itself.
+
+Runs the reference's own leap-frog path, compiled unmodified by
+oracle/Makefile against the project's Eigen-subset shim
+(oracle/_ref/tsp_ref_run), on small seeded meshes, and stores inputs and
+outputs as .npz. Rebuild with:
+
+    make -C oracle REF=/root/reference && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import zlib
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from tspeed_b200 import workloads as W  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "tsp_ref_run")
+
+# name: (nx, ny, Lx, Ly, N, materials, penalty, dt, nsteps, src, ricker(f0,t0,amp,dir), nrcv, dump_blocks)
+CASES = {
+    "g_n2_layers": dict(nx=6, ny=4, Lx=600.0, Ly=400.0, N=2, mat="layers", penalty=10.0, dt=4e-4, nsteps=60,
+                        src=(310.0, 190.0), ricker=(15.0, 1 / 15.0, -1.0, 1), nrcv=4, blocks=True),
+    "g_n4_lognormal": dict(nx=8, ny=5, Lx=800.0, Ly=500.0, N=4, mat="lognormal", penalty=10.0, dt=1.5e-4,
+                           nsteps=40, src=(400.0, 260.0), ricker=(12.0, 1 / 12.0, -1.0, 1), nrcv=5, blocks=False),
+    "g_config1_small": dict(nx=10, ny=5, Lx=4000.0, Ly=2000.0, N=4, mat="config1", penalty=10.0, dt=2e-3,
+                            nsteps=150, src=(2000.0, 1500.0), ricker=(8.0, 1 / 8.0, -1.0, 1), nrcv=8, blocks=False),
+    "g_n1_xforce": dict(nx=4, ny=3, Lx=400.0, Ly=300.0, N=1, mat="homog", penalty=2.0, dt=1e-3, nsteps=50,
+                        src=(150.0, 140.0), ricker=(10.0, 0.1, 1.0, 0), nrcv=3, blocks=True),
+    "g_n8": dict(nx=3, ny=2, Lx=300.0, Ly=200.0, N=8, mat="lognormal", penalty=10.0, dt=2e-5, nsteps=20,
+                 src=(140.0, 90.0), ricker=(20.0, 0.05, -1.0, 1), nrcv=2, blocks=False),
+}
+
+
+def materials(kind, m, rng):
+    ne = m.ne
+    if kind == "layers":
+        top = W.centroids(m)[:, 1] > 0.6 * m.Ly
+        m.region = np.where(top, 1, 2).astype(np.int32)
+        return W.lame(np.where(top, 1800.0, 4000.0), np.where(top, 1000.0, 2300.0), np.where(top, 1900.0, 2500.0))
+    if kind == "lognormal":
+        vp = 3000 * np.exp(rng.normal(0, 0.1, ne))
+        return W.lame(vp, vp / np.sqrt(3), 2000 + 300 * rng.random(ne))
+    if kind == "config1":
+        return W.lame(np.full(ne, 3200.0), np.full(ne, 1847.0), np.full(ne, 2200.0))
+    return W.lame(np.full(ne, 3000.0), np.full(ne, 1700.0), np.full(ne, 2100.0))
+
+
+def run_case(name, c, tmp):
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    m = W.jittered_rect(c["nx"], c["ny"], c["Lx"], c["Ly"], seed=11)
+    lam, mu, rho = materials(c["mat"], m, rng)
+    rcv = W.surface_receivers(m, c["nrcv"])
+    msh, rcvf, matf, out = (os.path.join(tmp, name + s) for s in (".msh", ".rcv", ".mat", ""))
+    W.write_gmsh(msh, m)
+    W.write_rcv(rcvf, rcv)
+    np.stack([lam, mu, rho], 1).astype(np.float64).tofile(matf)
+    f0, t0, amp, sdir = c["ricker"]
+    cmd = [REF, "--mesh", msh, "--N", str(c["N"]), "--mat", matf, "--rcv", rcvf, "--out", out, "--dt", repr(c["dt"]),
+           "--nsteps", str(c["nsteps"]), "--src", repr(c["src"][0]), repr(c["src"][1]), "--ricker", repr(f0),
+           repr(t0), repr(amp), "--sdir", str(sdir), "--penalty", repr(c["penalty"])]
+    if c["blocks"]:
+        cmd.append("--dump-blocks")
+    info = json.loads(subprocess.run(cmd, check=True, capture_output=True, text=True).stdout)
+    ne = m.ne
+    raw = open(out + ".mesh.bin", "rb").read()
+    off = 0
+    hdr = np.frombuffer(raw, np.int32, 2, off); off += 8
+    Np = int(hdr[1])
+    nb = np.frombuffer(raw, np.int32, ne * 6, off).reshape(ne, 6); off += ne * 24
+    geo = np.frombuffer(raw, np.float64, ne * 5, off).reshape(ne, 5); off += ne * 40
+    minv = np.frombuffer(raw, np.float64, ne, off); off += ne * 8
+    src_elem = int(np.frombuffer(raw, np.int32, 1, off)[0]); off += 4
+    src_phi = np.frombuffer(raw, np.float64, Np, off); off += Np * 8
+    nr = int(np.frombuffer(raw, np.int32, 1, off)[0]); off += 4
+    rcv_elem, rcv_phi = [], []
+    for _ in range(nr):
+        rcv_elem.append(int(np.frombuffer(raw, np.int32, 1, off)[0])); off += 4
+        rcv_phi.append(np.frombuffer(raw, np.float64, Np, off)); off += Np * 8
+    u = open(out + ".u.bin", "rb").read()
+    rec = 8 + 16 * ne * Np
+    snaps = {int(np.frombuffer(u, np.int64, 1, i)[0]): np.frombuffer(u, np.float64, 2 * ne * Np, i + 8)
+             for i in range(0, len(u), rec)}
+    seis = np.fromfile(out + ".seis.bin", dtype=np.float64).reshape(c["nsteps"], nr, 2)
+    d = dict(xy=m.xy, tri=m.tri, region=m.region, lam=lam, mu=mu, rho=rho, N=c["N"], penalty=c["penalty"],
+             dt=c["dt"], nsteps=c["nsteps"], src=np.array(c["src"]), ricker=np.array(c["ricker"]),
+             rcv=np.array(rcv), neigh=nb[:, :3], nedge=nb[:, 3:], detJ=geo[:, 0], minv=minv, src_elem=src_elem,
+             src_phi=src_phi, rcv_elem=np.array(rcv_elem), rcv_phi=np.array(rcv_phi), seis=seis,
+             u_first=snaps[1], u_final=snaps[c["nsteps"]], last_time=info["last_time"])
+    if c["blocks"]:
+        b = open(out + ".blocks.bin", "rb").read()
+        h = np.frombuffer(b, np.int32, 3, 0)
+        nnzb = int(h[2])
+        o = 12
+        d["row_ptr"] = np.frombuffer(b, np.int32, ne + 1, o); o += 4 * (ne + 1)
+        d["col"] = np.frombuffer(b, np.int32, nnzb, o); o += 4 * nnzb
+        d["blocks"] = np.frombuffer(b, np.float64, nnzb * 4 * Np * Np, o).reshape(nnzb, 2 * Np, 2 * Np)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
+    print(name, "ne", ne, "Np", Np, "steps", c["nsteps"], "last_time", info["last_time"])
+
+
+def main():
+    if not os.path.exists(REF):
+        sys.exit(f"{REF} missing: run `make -C oracle REF=/root/reference` first")
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, c in CASES.items():
+            run_case(name, c, tmp)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,116 @@
+"""Engine features beyond parity: graphs, energy, checkpoint/resume, CFL
+estimate, watchdog and error codes (GPU)."""
+import numpy as np
+import pytest
+
+import tsp_oracle as O
+from helpers import rel
+from tspeed_b200 import capi
+from tspeed_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def small(N=3, nx=6, ny=4, precision="fp64", nshots=1):
+    m = W.jittered_rect(nx, ny, 100.0 * nx, 100.0 * ny, seed=5)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    shots = [(0.4 * m.Lx + 10 * k, 0.5 * m.Ly) for k in range(nshots)]
+    s = capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, W.surface_receivers(m, 3), penalty=10.0,
+                               precision=precision)
+    return m, (lam, mu, rho), s
+
+
+def test_graph_run_equals_single_steps():
+    _, _, a = small()
+    _, _, b = small()
+    for s in (a, b):
+        s.set_dt(1e-4)
+        s.set_ricker(0, 20.0, 0.05, -1.0, 1, 200)
+        s.first_step()
+    a.run(37)
+    a.run(37)
+    a.run(1)
+    for _ in range(75):
+        b.step()
+    assert np.array_equal(a.u(), b.u())
+    assert np.array_equal(a.seismograms(0, 76), b.seismograms(0, 76))
+    assert a.progress() == b.progress()
+
+
+def test_energy_conserved_without_force():
+    m, mat, s = small(N=4)
+    rng = np.random.default_rng(3)
+    u0 = 1e-3 * rng.standard_normal(2 * m.ne * s.Np)
+    lmax = s.estimate_lmax(200)
+    dt = 0.5 * 2 / np.sqrt(lmax)
+    s.set_dt(dt)
+    s.set_initial(0, u0, None)
+    s.enable_energy(True)
+    s.first_step()
+    s.run(299)
+    E = s.energy(0, 300)
+    assert np.all(np.isfinite(E)) and E[0] > 0
+    assert np.max(np.abs(E - E[0])) / E[0] < 1e-10
+
+
+def test_lmax_matches_dense_eigenvalue():
+    m, (lam, mu, rho), s = small(N=2, nx=4, ny=3)
+    est = s.estimate_lmax(2000)
+    sp = O.make_space(2)
+    tri = m.tri.astype(np.int64)
+    geo = O.geometry(m.xy, tri)
+    nb, ned = O.neighbours(tri)
+    row_ptr, cols, blocks, minv = O.assemble(sp, geo, nb, ned, lam, mu, rho, 10.0)
+    n = 2 * m.ne * sp.Np
+    Bd = np.stack([O.apply_B(row_ptr, cols, blocks, e, m.ne, sp.Np) for e in np.eye(n)], 1)
+    mv = np.concatenate([np.repeat(minv, sp.Np)] * 2)
+    true = np.max(np.linalg.eigvals(mv[:, None] * Bd).real)
+    assert abs(est - true) / true < 1e-6
+
+
+def test_checkpoint_resume_bit_exact():
+    _, _, a = small(nshots=2)
+    _, _, b = small(nshots=2)
+    for s in (a, b):
+        s.set_dt(1e-4)
+        for k in range(2):
+            s.set_ricker(k, 20.0, 0.05, -1.0, 1, 100)
+    a.first_step()
+    a.run(20)
+    up, uc, k, t = a.get_state()
+    b.set_state(up, uc, k, t)
+    a.run(30)
+    b.run(30)
+    assert np.array_equal(a.u(0), b.u(0)) and np.array_equal(a.u(1), b.u(1))
+    assert a.progress() == b.progress()
+
+
+def test_nonfinite_watchdog():
+    m, _, s = small()
+    s.set_dt(1e-4)
+    s.first_step()
+    assert s.check_finite()
+    up, uc, k, t = s.get_state()
+    uc[0, 5] = np.nan
+    s.set_state(up, uc, k, t)
+    assert not s.check_finite()
+
+
+def test_error_codes():
+    m, (lam, mu, rho), s = small()
+    with pytest.raises(capi.TspError) as e:
+        s.step()
+    assert e.value.code == -4  # step before first_step
+    with pytest.raises(capi.TspError) as e:
+        s.first_step()
+    assert e.value.code == -4  # no dt
+    with pytest.raises(capi.TspError) as e:
+        capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, [(-50.0, 10.0)], [])
+    assert e.value.code == -5  # source outside the mesh
+    cw = m.tri.copy()
+    cw[0] = cw[0][::-1]
+    with pytest.raises(capi.TspError) as e:
+        capi.Simulation.create(m.xy, cw, 3, lam, mu, rho, [(250.0, 200.0)], [])
+    assert e.value.code == -6  # clockwise triangle
+    with pytest.raises(capi.TspError):
+        s.seismograms(0, 10 ** 9)

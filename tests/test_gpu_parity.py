@@ -1,0 +1,143 @@
+"""Parity of the CUDA path against the reference's golden vectors and the
+oracle (GPU). Tolerances: 1e-12 relative for FP64; FP32/BF16 operators are
+checked against the FP64 path with the tolerances written below."""
+import numpy as np
+import pytest
+
+import tsp_oracle as O
+from helpers import oracle_setup, rel
+from tspeed_b200 import capi
+from tspeed_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def sim_from_golden(g, precision="fp64", shots=None):
+    src = [tuple(g["src"])] if shots is None else shots
+    s = capi.Simulation.create(g["xy"], g["tri"], int(g["N"]), g["lam"], g["mu"], g["rho"], src, g["rcv"],
+                               penalty=float(g["penalty"]), precision=precision)
+    s.set_dt(float(g["dt"]))
+    f0, t0, amp, sdir = g["ricker"]
+    for k in range(s.nshots):
+        s.set_ricker(k, f0, t0, amp, int(sdir), int(g["nsteps"]))
+    return s
+
+
+def finite_rel(a, b):
+    ok = np.isfinite(b)
+    return rel(a[ok], b[ok])
+
+
+def test_golden_run_through_device_assembly(golden):
+    """Mesh -> device assembly -> first_step + (n-1) steps vs the reference."""
+    g = golden
+    with sim_from_golden(g) as s:
+        s.first_step()
+        u1 = s.u()
+        s.run(int(g["nsteps"]) - 1)
+        u = s.u()
+        seis = s.seismograms(0, int(g["nsteps"]))[0]
+        k, t = s.progress()
+    assert rel(u1, g["u_first"]) < 1e-13
+    assert rel(u, g["u_final"]) < 1e-12
+    assert finite_rel(seis, g["seis"]) < 1e-12
+    # The product evaluates the basis at the collapsed vertex by its limit
+    # where the reference yields NaN.
+    assert np.isfinite(seis).all()
+    assert k == int(g["nsteps"]) and t == float(g["last_time"])
+
+
+def test_golden_operator_export(golden):
+    g = golden
+    o = oracle_setup(g)
+    with sim_from_golden(g) as s:
+        row_ptr, col, blocks, minv = s.export_operator()
+        se, sp, re_, rp = s.export_points()
+    assert np.array_equal(row_ptr, o["row_ptr"]) and np.array_equal(col, o["cols"])
+    ref = g["blocks"] if "blocks" in g else o["blocks"]
+    assert np.abs(blocks - ref).max() / np.abs(ref).max() < 1e-13
+    assert np.array_equal(minv, g["minv"])
+    assert se[0] == int(g["src_elem"]) and list(re_) == list(g["rcv_elem"])
+    assert np.allclose(sp[0], g["src_phi"], rtol=0, atol=1e-13)
+    ok = np.isfinite(g["rcv_phi"])
+    assert np.allclose(rp[ok], g["rcv_phi"][ok], rtol=0, atol=1e-13)
+
+
+def test_golden_run_from_reference_blocks(golden):
+    """The drop-in boundary fed with the reference's own assembled B."""
+    g = golden
+    if "blocks" not in g:
+        pytest.skip("case without block dump")
+    rphi = np.nan_to_num(g["rcv_phi"])
+    f0, t0, amp, sdir = g["ricker"]
+    with capi.Simulation.from_blocks(g["row_ptr"], g["col"], g["blocks"], g["minv"], [int(g["src_elem"])],
+                                     g["src_phi"][None], g["rcv_elem"], rphi) as s:
+        s.set_dt(float(g["dt"]))
+        s.set_ricker(0, f0, t0, amp, int(sdir), int(g["nsteps"]))
+        s.first_step()
+        for _ in range(int(g["nsteps"]) - 1):
+            s.step()
+        u = s.u()
+        seis = s.seismograms(0, int(g["nsteps"]))[0]
+    assert rel(u, g["u_final"]) < 1e-12
+    assert finite_rel(seis, g["seis"]) < 1e-12
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_apply_matches_oracle_all_degrees(N):
+    m = W.jittered_rect(5, 4, 500.0, 400.0, seed=N)
+    rng = np.random.default_rng(N)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    sp = O.make_space(N)
+    tri = m.tri.astype(np.int64)
+    geo = O.geometry(m.xy, tri)
+    nb, ned = O.neighbours(tri)
+    row_ptr, cols, blocks, minv = O.assemble(sp, geo, nb, ned, lam, mu, rho, 10.0)
+    x = rng.standard_normal(2 * m.ne * sp.Np)
+    y_ref = O.apply_B(row_ptr, cols, blocks, x, m.ne, sp.Np)
+    with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, [(250.0, 200.0)], [], penalty=10.0) as s:
+        y = s.apply(x)
+    assert rel(y, y_ref) < 1e-13
+
+
+def test_multishot_matches_single_shots():
+    g = oracle_case = None  # noqa: F841
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=21)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    shots = [(150.0, 120.0), (420.0, 300.0), (305.0, 205.0)]
+    rcv = W.surface_receivers(m, 4)
+    N, dt, n = 3, 2e-4, 40
+    outs = []
+    with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0) as s:
+        s.set_dt(dt)
+        for k in range(3):
+            s.set_ricker(k, 15.0, 1 / 15.0, -1.0, 1, n)
+        s.first_step()
+        s.run(n - 1)
+        multi = [s.u(k) for k in range(3)]
+        mseis = s.seismograms(0, n)
+    for k, sh in enumerate(shots):
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, [sh], rcv, penalty=10.0) as s:
+            s.set_dt(dt)
+            s.set_ricker(0, 15.0, 1 / 15.0, -1.0, 1, n)
+            s.first_step()
+            s.run(n - 1)
+            assert rel(multi[k], s.u()) < 1e-14
+            assert rel(mseis[k], s.seismograms(0, n)[0]) < 1e-14
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-4), ("bf16", 5e-2)])
+def test_mixed_precision_close_to_fp64(precision, tol):
+    g = __import__("conftest").load_golden("g_config1_small")
+    with sim_from_golden(g, "fp64") as s:
+        s.first_step()
+        s.run(int(g["nsteps"]) - 1)
+        ref = s.seismograms(0, int(g["nsteps"]))[0]
+    with sim_from_golden(g, precision) as s:
+        s.first_step()
+        s.run(int(g["nsteps"]) - 1)
+        lo = s.seismograms(0, int(g["nsteps"]))[0]
+    err = rel(lo, ref)
+    print(precision, "seismogram rel L2 error vs fp64:", err)
+    assert err < tol

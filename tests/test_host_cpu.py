@@ -1,0 +1,89 @@
+"""Host-side checks of the C-ABI library that need no GPU (CPU)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import tsp_oracle as O
+from tspeed_b200 import capi
+from tspeed_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    syms = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(inc, fn)).read()
+            syms |= set(re.findall(r"^\w[\w\s\*]*?\b(tsp_\w+)\s*\(", txt, flags=re.M))
+    return syms
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    syms = header_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(capi.SIGNATURES) == syms
+
+
+def test_version_string():
+    assert b"sm_100a" in capi.lib().tsp_version()
+
+
+def test_gmsh_roundtrip(tmp_path):
+    m = W.jittered_rect(5, 3, 500.0, 300.0, seed=4)
+    m.region = (1 + (np.arange(m.ne) % 3)).astype(np.int32)
+    p = str(tmp_path / "m.msh")
+    W.write_gmsh(p, m)
+    xy, tri, reg = capi.gmsh_read(p)
+    assert np.array_equal(xy, m.xy) and np.array_equal(tri, m.tri) and np.array_equal(reg, m.region)
+
+
+def test_gmsh_errors(tmp_path):
+    with pytest.raises(capi.TspError) as e:
+        capi.gmsh_read(str(tmp_path / "missing.msh"))
+    assert e.value.code == -6
+    bad = tmp_path / "bad.msh"
+    bad.write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n")
+    with pytest.raises(capi.TspError):
+        capi.gmsh_read(str(bad))
+
+
+def test_neighbours_match_oracle_and_golden(golden):
+    nb, ned = capi.mesh_neighbours(golden["tri"])
+    assert np.array_equal(nb, golden["neigh"]) and np.array_equal(ned, golden["nedge"])
+
+
+def test_neighbours_large_mesh_matches_oracle():
+    m = W.jittered_rect(60, 40, 6000.0, 4000.0, seed=9)
+    nb, ned = capi.mesh_neighbours(m.tri)
+    onb, oned = O.neighbours(m.tri.astype(np.int64))
+    assert np.array_equal(nb, onb) and np.array_equal(ned, oned)
+
+
+def test_neighbours_reject_clockwise_duplicate():
+    tri = np.array([[0, 1, 2], [0, 1, 3]], dtype=np.int32)  # both own directed edge 0->1
+    with pytest.raises(capi.TspError) as e:
+        capi.mesh_neighbours(tri)
+    assert e.value.code == -6
+
+
+def test_force_times_match_oracle():
+    for dt in (1e-3, 3.7e-4, 0.1):
+        assert np.array_equal(capi.force_times(dt, 500), np.array(O.force_times(dt, 500)))
+
+
+def test_create_validates_before_touching_a_device():
+    m = W.jittered_rect(2, 2, 200.0, 200.0, seed=1)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1700.0), np.full(m.ne, 2000.0))
+    with pytest.raises(capi.TspError) as e:
+        capi.Simulation.create(m.xy, m.tri, 0, lam, mu, rho, [(50.0, 50.0)], [])
+    assert e.value.code == -9
+    with pytest.raises(capi.TspError) as e:
+        capi.Simulation.create(m.xy, m.tri, 3, lam, mu, -rho, [(50.0, 50.0)], [])
+    assert e.value.code == -1

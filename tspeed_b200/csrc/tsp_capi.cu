@@ -1,0 +1,970 @@
+// C-ABI of the tspeed_b200 engine (include/tspeed_b200.h).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/tspeed_b200.h"
+#include "tsp_host.h"
+#include "tsp_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_create_error = "no error";
+
+}  // namespace
+
+struct tsp_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int ne = 0, N = 0, Np = 0, R = 0, S = 1, nrcv = 0;
+  long long nnzb = 0;
+  int prec = TSP_PREC_FP64, op_kind = TSP_OP_EXPLICIT;
+  // operator
+  int* d_row_ptr = nullptr;
+  int* d_col = nullptr;
+  void* d_blocks = nullptr;
+  float* d_bscale = nullptr;
+  double* d_minv = nullptr;
+  // state
+  double* d_U[2] = {nullptr, nullptr};
+  int cur = 0;  // d_U[cur] holds u^k, d_U[1-cur] holds u^{k-1}
+  double* d_v0 = nullptr;
+  long long* d_step = nullptr;
+  // sources / receivers
+  int* d_src_elem = nullptr;
+  double* d_src_phi = nullptr;
+  double* d_F = nullptr;
+  long long nF = 0;
+  int* d_rcv_ptr = nullptr;
+  int* d_rcv_id = nullptr;
+  double* d_rcv_phi = nullptr;
+  double* d_seis = nullptr;
+  long long seis_cap = 0;
+  double* d_energy = nullptr;
+  long long energy_cap = 0;
+  bool energy_on = false;
+  double* d_acc = nullptr;
+  // host mirrors
+  std::vector<int> src_elem, rcv_elem;
+  std::vector<double> src_phi, rcv_phi, Fhost;
+  double dt = 0.0;
+  bool dt_set = false;
+  long long steps_done = 0;
+  double last_time = 0.0;
+  std::string err = "no error";
+  std::map<std::pair<long long, int>, cudaGraphExec_t> graphs;
+  std::vector<void*> owned;  // device allocations, freed at destroy
+};
+
+namespace {
+
+int fail(tsp_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+#define TSP_CUDA(h, call)                                                                          \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail((h), e_ == cudaErrorMemoryAllocation ? TSP_ERR_NOMEM : TSP_ERR_CUDA,             \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                             \
+  } while (0)
+
+template <typename T>
+int dalloc(tsp_handle* h, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(h, TSP_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) + " bytes: " +
+                                      cudaGetErrorString(e));
+  h->owned.push_back(*p);
+  return TSP_OK;
+}
+
+void dfree(tsp_handle* h, void* p) {
+  if (!p) return;
+  auto it = std::find(h->owned.begin(), h->owned.end(), p);
+  if (it != h->owned.end()) h->owned.erase(it);
+  cudaFree(p);
+}
+
+template <typename T>
+int upload(tsp_handle* h, T** d, const T* src, size_t n) {
+  int rc = dalloc(h, d, n);
+  if (rc) return rc;
+  if (n) TSP_CUDA(h, cudaMemcpyAsync(*d, src, n * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  return TSP_OK;
+}
+
+void clear_graphs(tsp_handle* h) {
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+}
+
+// Receivers sorted by element into a CSR over elements.
+int build_receiver_csr(tsp_handle* h) {
+  if (h->nrcv == 0) return TSP_OK;
+  std::vector<int> ptr(size_t(h->ne) + 1, 0), ids(h->nrcv);
+  for (int r = 0; r < h->nrcv; ++r) ptr[h->rcv_elem[r] + 1]++;
+  for (int e = 0; e < h->ne; ++e) ptr[e + 1] += ptr[e];
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (int r = 0; r < h->nrcv; ++r) ids[fill[h->rcv_elem[r]]++] = r;
+  int rc;
+  if ((rc = upload(h, &h->d_rcv_ptr, ptr.data(), ptr.size()))) return rc;
+  if ((rc = upload(h, &h->d_rcv_id, ids.data(), ids.size()))) return rc;
+  if ((rc = upload(h, &h->d_rcv_phi, h->rcv_phi.data(), h->rcv_phi.size()))) return rc;
+  return TSP_OK;
+}
+
+int alloc_seis(tsp_handle* h, long long cap) {
+  dfree(h, h->d_seis);
+  h->d_seis = nullptr;
+  h->seis_cap = cap;
+  if (h->nrcv == 0) return TSP_OK;
+  int rc = dalloc(h, &h->d_seis, size_t(h->S) * size_t(cap) * h->nrcv * 2);
+  if (rc) return rc;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_seis, 0, size_t(h->S) * size_t(cap) * h->nrcv * 2 * sizeof(double), h->stream));
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+// Common tail of both constructors: state, step counter, sources, receivers.
+int finish_create(tsp_handle* h) {
+  int rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = dalloc(h, &h->d_U[i], nstate))) return rc;
+    TSP_CUDA(h, cudaMemsetAsync(h->d_U[i], 0, nstate * sizeof(double), h->stream));
+  }
+  if ((rc = dalloc(h, &h->d_step, 1))) return rc;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  if ((rc = dalloc(h, &h->d_acc, 3))) return rc;
+  if ((rc = upload(h, &h->d_src_elem, h->src_elem.data(), h->src_elem.size()))) return rc;
+  if ((rc = upload(h, &h->d_src_phi, h->src_phi.data(), h->src_phi.size()))) return rc;
+  if ((rc = build_receiver_csr(h))) return rc;
+  long long cap = 4096;
+  if (h->nrcv > 0) {
+    const long long per = (long long)h->S * h->nrcv * 16;
+    cap = std::max<long long>(1, std::min<long long>(4096, (256ll << 20) / per));
+  }
+  if ((rc = alloc_seis(h, cap))) return rc;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TSP_OK;
+}
+
+template <int R>
+int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::RowTeam<R, double> RT;
+  const long long teams = (long long)h->ne * h->S;
+  const unsigned grid = unsigned((teams + RT::TEAMS_PER_CTA - 1) / RT::TEAMS_PER_CTA);
+  switch (h->prec) {
+    case TSP_PREC_FP64: tsp::k_step_rows<R, double><<<grid, RT::THREADS, 0, st>>>(p); break;
+    case TSP_PREC_FP32: tsp::k_step_rows<R, float><<<grid, RT::THREADS, 0, st>>>(p); break;
+    default: tsp::k_step_rows<R, __nv_bfloat16><<<grid, RT::THREADS, 0, st>>>(p); break;
+  }
+  return TSP_OK;
+}
+
+int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, double* out, int rel,
+                double xscale, cudaStream_t st) {
+  tsp::StepParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.ne = h->ne;
+  p.S = h->S;
+  p.mode = mode;
+  p.row_ptr = h->d_row_ptr;
+  p.col = h->d_col;
+  p.blocks = h->d_blocks;
+  p.bscale = (h->prec == TSP_PREC_BF16) ? h->d_bscale : nullptr;
+  p.minv = h->d_minv;
+  p.x = x;
+  p.uprev = uprev;
+  p.out = out;
+  p.dt = h->dt;
+  p.xscale = xscale;
+  p.step_base = h->d_step;
+  p.rel = rel;
+  p.src_elem = h->d_src_elem;
+  p.src_phi = h->d_src_phi;
+  p.F = h->d_F;
+  p.nF = h->d_F ? h->nF : 0;
+  const bool sample = (mode == tsp::kModeStep || mode == tsp::kModeFirst);
+  p.rcv_ptr = (sample && h->nrcv > 0) ? h->d_rcv_ptr : nullptr;
+  p.rcv_id = h->d_rcv_id;
+  p.rcv_phi = h->d_rcv_phi;
+  p.seis = h->d_seis;
+  p.nrcv = h->nrcv;
+  p.seis_cap = h->seis_cap;
+  p.energy = (sample && h->energy_on) ? h->d_energy : nullptr;
+  p.energy_cap = h->energy_cap;
+  p.acc = h->d_acc;
+  switch (h->R) {
+    case 6: return launch_R<6>(h, p, st);
+    case 12: return launch_R<12>(h, p, st);
+    case 20: return launch_R<20>(h, p, st);
+    case 30: return launch_R<30>(h, p, st);
+    case 42: return launch_R<42>(h, p, st);
+    case 56: return launch_R<56>(h, p, st);
+    case 72: return launch_R<72>(h, p, st);
+    case 90: return launch_R<90>(h, p, st);
+    default: return fail(h, TSP_ERR_UNSUPPORTED, "no kernel for 2Np = " + std::to_string(h->R));
+  }
+}
+
+// Reference layout u[c*ne*Np + e*Np + i] <-> device layout [(e*S+s)*R + c*Np + i].
+void ref_to_dev(const tsp_handle* h, int shot, const double* src, double* dst_all) {
+  const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
+  for (int e = 0; e < ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(dst_all + (size_t(e) * S + shot) * R + size_t(c) * Np, src + size_t(c) * ne * Np + size_t(e) * Np,
+                  Np * sizeof(double));
+}
+void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* dst) {
+  const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
+  for (int e = 0; e < ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(dst + size_t(c) * ne * Np + size_t(e) * Np, src_all + (size_t(e) * S + shot) * R + size_t(c) * Np,
+                  Np * sizeof(double));
+}
+
+
+int begin(tsp_handle* h) {
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return TSP_OK;
+}
+
+int make_handle(int device, tsp_handle** out) {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, TSP_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= ndev) return fail(nullptr, TSP_ERR_ARG, "device ordinal out of range");
+  tsp_handle* h = new tsp_handle();
+  h->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    return fail(nullptr, TSP_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return TSP_OK;
+}
+
+int create_error_from(tsp_handle* h, int rc) {
+  g_create_error = h->err;
+  tsp_destroy(h);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tsp_version(void) { return "tspeed_b200 0.1 sm_100a"; }
+
+const char* tsp_last_error(const tsp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int tsp_create(const tsp_problem* P, tsp_handle** out) {
+  if (!P || !out) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (P->N < 1 || P->N > tsp::kMaxN) return fail(nullptr, TSP_ERR_UNSUPPORTED, "degree N must be in 1..8");
+  if (P->ne <= 0 || P->nverts <= 0 || !P->xy || !P->tri || !P->lambda || !P->mu || !P->rho)
+    return fail(nullptr, TSP_ERR_ARG, "mesh or material arrays missing");
+  if (P->nshots < 1 || !P->src_xy) return fail(nullptr, TSP_ERR_ARG, "need nshots >= 1 and src_xy");
+  if (P->nrcv < 0 || (P->nrcv > 0 && !P->rcv_xy)) return fail(nullptr, TSP_ERR_ARG, "bad receivers");
+  if (P->precision < TSP_PREC_FP64 || P->precision > TSP_PREC_BF16) return fail(nullptr, TSP_ERR_ARG, "bad precision");
+  if (P->op_kind != TSP_OP_EXPLICIT)
+    return fail(nullptr, TSP_ERR_UNSUPPORTED, "matrix-free operator not available in this build");
+  for (int32_t i = 0; i < 3 * P->ne; ++i)
+    if (P->tri[i] < 0 || P->tri[i] >= P->nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  for (int32_t e = 0; e < P->ne; ++e)
+    if (!(P->rho[e] > 0) || !(P->mu[e] >= 0) || !std::isfinite(P->lambda[e]))
+      return fail(nullptr, TSP_ERR_ARG, "material values must be finite with rho > 0, mu >= 0");
+
+  tsp_handle* h = nullptr;
+  int rc = make_handle(P->device, &h);
+  if (rc) return rc;
+  h->ne = P->ne;
+  h->N = P->N;
+  h->Np = tsp::np_of(P->N);
+  h->R = 2 * h->Np;
+  h->S = P->nshots;
+  h->nrcv = P->nrcv;
+  h->prec = P->precision;
+  h->op_kind = P->op_kind;
+
+  // ---- host setup: geometry, neighbours, pattern, tables ----
+  tsp::Geometry g = tsp::make_geometry(P->ne, P->xy, P->tri);
+  for (int32_t e = 0; e < P->ne; ++e)
+    if (!(g.detJ[e] > 0)) {
+      fail(h, TSP_ERR_MESH, "element " + std::to_string(e) +
+                                " is clockwise or degenerate (detJ <= 0); the signed-detJ mass of "
+                                "Matrices_imp.hpp:186-189 would be non-positive");
+      return create_error_from(h, TSP_ERR_MESH);
+    }
+  std::vector<int32_t> neigh(size_t(P->ne) * 3), nedge(size_t(P->ne) * 3);
+  std::string err;
+  if (!tsp::build_neighbours(P->ne, P->tri, neigh.data(), nedge.data(), &err)) {
+    fail(h, TSP_ERR_MESH, err);
+    return create_error_from(h, TSP_ERR_MESH);
+  }
+  std::vector<int32_t> row_ptr, col;
+  std::vector<int8_t> bface;
+  tsp::bsr_pattern(P->ne, neigh.data(), &row_ptr, &col, &bface);
+  h->nnzb = (long long)col.size();
+  tsp::RefTables T = tsp::make_tables(P->N);
+
+  // ---- sources and receivers ----
+  h->src_elem.resize(h->S);
+  h->src_phi.resize(size_t(h->S) * h->Np);
+  for (int s = 0; s < h->S; ++s) {
+    const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->src_xy[2 * s], P->src_xy[2 * s + 1],
+                                    &h->src_phi[size_t(s) * h->Np]);
+    if (e < 0) {
+      fail(h, TSP_ERR_NOT_FOUND, "source point " + std::to_string(s) + " not found in the mesh");
+      return create_error_from(h, TSP_ERR_NOT_FOUND);
+    }
+    h->src_elem[s] = e;
+  }
+  h->rcv_elem.resize(h->nrcv);
+  h->rcv_phi.resize(size_t(h->nrcv) * h->Np);
+  for (int r = 0; r < h->nrcv; ++r) {
+    const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->rcv_xy[2 * r], P->rcv_xy[2 * r + 1],
+                                    &h->rcv_phi[size_t(r) * h->Np]);
+    if (e < 0) {
+      fail(h, TSP_ERR_NOT_FOUND, "receiver point " + std::to_string(r) + " not found in the mesh");
+      return create_error_from(h, TSP_ERR_NOT_FOUND);
+    }
+    h->rcv_elem[r] = e;
+  }
+
+  // ---- device upload + assembly ----
+  std::vector<double> minv(P->ne);
+  for (int32_t e = 0; e < P->ne; ++e) minv[e] = (1. / P->rho[e]) / g.detJ[e];  // Matrices_imp.hpp:187
+  int* d_neigh = nullptr;
+  int* d_nedge = nullptr;
+  signed char* d_bface = nullptr;
+  double *d_invJ = nullptr, *d_detJ = nullptr, *d_elen = nullptr, *d_enrm = nullptr, *d_lam = nullptr,
+         *d_mu = nullptr, *d_K = nullptr, *d_Ws = nullptr, *d_Wx = nullptr, *d_Ds = nullptr, *d_Dx = nullptr;
+  if ((rc = upload(h, &h->d_row_ptr, row_ptr.data(), row_ptr.size())) ||
+      (rc = upload(h, &h->d_col, col.data(), col.size())) || (rc = upload(h, &h->d_minv, minv.data(), minv.size())) ||
+      (rc = upload(h, &d_neigh, neigh.data(), neigh.size())) ||
+      (rc = upload(h, &d_nedge, nedge.data(), nedge.size())) ||
+      (rc = upload(h, &d_bface, reinterpret_cast<const signed char*>(bface.data()), bface.size())) ||
+      (rc = upload(h, &d_invJ, g.invJ.data(), g.invJ.size())) ||
+      (rc = upload(h, &d_detJ, g.detJ.data(), g.detJ.size())) ||
+      (rc = upload(h, &d_elen, g.elen.data(), g.elen.size())) ||
+      (rc = upload(h, &d_enrm, g.enrm.data(), g.enrm.size())) || (rc = upload(h, &d_lam, P->lambda, size_t(P->ne))) ||
+      (rc = upload(h, &d_mu, P->mu, size_t(P->ne))) || (rc = upload(h, &d_K, T.K.data(), T.K.size())) ||
+      (rc = upload(h, &d_Ws, T.Ws.data(), T.Ws.size())) || (rc = upload(h, &d_Wx, T.Wx.data(), T.Wx.size())) ||
+      (rc = upload(h, &d_Ds, T.Ds.data(), T.Ds.size())) || (rc = upload(h, &d_Dx, T.Dx.data(), T.Dx.size())))
+    return create_error_from(h, rc);
+  const size_t RR = size_t(h->R) * h->R;
+  const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
+  {
+    void* blk = nullptr;
+    cudaError_t ce = cudaMalloc(&blk, size_t(h->nnzb) * RR * esz);
+    if (ce != cudaSuccess) {
+      fail(h, TSP_ERR_NOMEM, "operator blocks (" + std::to_string(size_t(h->nnzb) * RR * esz) +
+                                 " bytes) do not fit: " + cudaGetErrorString(ce));
+      return create_error_from(h, TSP_ERR_NOMEM);
+    }
+    h->owned.push_back(blk);
+    h->d_blocks = blk;
+  }
+  if (h->prec == TSP_PREC_BF16 && (rc = dalloc(h, &h->d_bscale, size_t(h->nnzb)))) return create_error_from(h, rc);
+  tsp::AssembleParams ap;
+  ap.ne = h->ne;
+  ap.N = h->N;
+  ap.Np = h->Np;
+  ap.pen_n2 = P->penalty * h->N * h->N;
+  ap.row_ptr = h->d_row_ptr;
+  ap.col = h->d_col;
+  ap.bface = d_bface;
+  ap.neigh = d_neigh;
+  ap.nedge = d_nedge;
+  ap.invJ = d_invJ;
+  ap.detJ = d_detJ;
+  ap.elen = d_elen;
+  ap.enrm = d_enrm;
+  ap.lam = d_lam;
+  ap.mu = d_mu;
+  ap.K = d_K;
+  ap.Ws = d_Ws;
+  ap.Wx = d_Wx;
+  ap.Ds = d_Ds;
+  ap.Dx = d_Dx;
+  ap.prec = h->prec;
+  ap.out = h->d_blocks;
+  ap.scale = h->d_bscale;
+  // Large meshes exceed the 2^31-1 grid limit only beyond 2 G blocks.
+  tsp::k_assemble<<<unsigned(h->nnzb), 256, 0, h->stream>>>(ap);
+  {
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) {
+      fail(h, TSP_ERR_CUDA, std::string("assembly kernel: ") + cudaGetErrorString(ce));
+      return create_error_from(h, TSP_ERR_CUDA);
+    }
+  }
+  for (void* q : {(void*)d_neigh, (void*)d_nedge, (void*)d_bface, (void*)d_invJ, (void*)d_detJ, (void*)d_elen,
+                  (void*)d_enrm, (void*)d_lam, (void*)d_mu, (void*)d_K, (void*)d_Ws, (void*)d_Wx, (void*)d_Ds,
+                  (void*)d_Dx})
+    dfree(h, q);
+  if ((rc = finish_create(h))) return create_error_from(h, rc);
+  *out = h;
+  return TSP_OK;
+}
+
+int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
+  if (!P || !out) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (P->ne <= 0 || P->Np <= 0 || P->nnzb < P->ne || !P->row_ptr || !P->col || !P->blocks || !P->minv)
+    return fail(nullptr, TSP_ERR_ARG, "operator arrays missing");
+  if (P->nshots < 1 || !P->src_elem || !P->src_phi) return fail(nullptr, TSP_ERR_ARG, "need nshots >= 1 sources");
+  if (P->nrcv < 0 || (P->nrcv > 0 && (!P->rcv_elem || !P->rcv_phi))) return fail(nullptr, TSP_ERR_ARG, "bad receivers");
+  if (P->precision < TSP_PREC_FP64 || P->precision > TSP_PREC_BF16) return fail(nullptr, TSP_ERR_ARG, "bad precision");
+  int N = -1;
+  for (int n = 1; n <= tsp::kMaxN; ++n)
+    if (tsp::np_of(n) == P->Np) N = n;
+  if (N < 0) return fail(nullptr, TSP_ERR_UNSUPPORTED, "Np must be (N+1)(N+2)/2 for N in 1..8");
+  if (P->row_ptr[0] != 0 || P->row_ptr[P->ne] != P->nnzb) return fail(nullptr, TSP_ERR_ARG, "row_ptr inconsistent");
+  for (int e = 0; e < P->ne; ++e) {
+    const int n = P->row_ptr[e + 1] - P->row_ptr[e];
+    if (n < 1 || n > 4) return fail(nullptr, TSP_ERR_ARG, "each block row needs 1..4 blocks");
+  }
+  for (int b = 0; b < P->nnzb; ++b)
+    if (P->col[b] < 0 || P->col[b] >= P->ne) return fail(nullptr, TSP_ERR_ARG, "block column out of range");
+  for (int s = 0; s < P->nshots; ++s)
+    if (P->src_elem[s] < 0 || P->src_elem[s] >= P->ne) return fail(nullptr, TSP_ERR_ARG, "source element out of range");
+  for (int r = 0; r < P->nrcv; ++r)
+    if (P->rcv_elem[r] < 0 || P->rcv_elem[r] >= P->ne) return fail(nullptr, TSP_ERR_ARG, "receiver element out of range");
+
+  tsp_handle* h = nullptr;
+  int rc = make_handle(P->device, &h);
+  if (rc) return rc;
+  h->ne = P->ne;
+  h->N = N;
+  h->Np = P->Np;
+  h->R = 2 * P->Np;
+  h->S = P->nshots;
+  h->nrcv = P->nrcv;
+  h->prec = P->precision;
+  h->nnzb = P->nnzb;
+  h->src_elem.assign(P->src_elem, P->src_elem + h->S);
+  h->src_phi.assign(P->src_phi, P->src_phi + size_t(h->S) * h->Np);
+  h->rcv_elem.assign(P->rcv_elem, P->rcv_elem + h->nrcv);
+  h->rcv_phi.assign(P->rcv_phi, P->rcv_phi + size_t(h->nrcv) * h->Np);
+  if ((rc = upload(h, &h->d_row_ptr, P->row_ptr, size_t(P->ne) + 1)) || (rc = upload(h, &h->d_col, P->col, size_t(P->nnzb))) ||
+      (rc = upload(h, &h->d_minv, P->minv, size_t(P->ne))))
+    return create_error_from(h, rc);
+  // Transpose every block to column-major and convert to the storage type.
+  const int R = h->R;
+  const size_t RR = size_t(R) * R;
+  const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
+  std::vector<unsigned char> host(size_t(P->nnzb) * RR * esz);
+  std::vector<float> scales(h->prec == TSP_PREC_BF16 ? size_t(P->nnzb) : 0);
+  for (int b = 0; b < P->nnzb; ++b) {
+    const double* src = P->blocks + size_t(b) * RR;
+    float sc = 1.0f;
+    if (h->prec == TSP_PREC_BF16) {
+      float m = 0.0f;
+      for (size_t t = 0; t < RR; ++t) m = std::max(m, float(std::fabs(src[t])));
+      sc = m > 0 ? std::exp2(std::ceil(std::log2(m))) : 1.0f;
+      scales[b] = sc;
+    }
+    for (int r = 0; r < R; ++r)
+      for (int c = 0; c < R; ++c) {
+        const double v = src[size_t(r) * R + c];
+        const size_t o = size_t(b) * RR + size_t(c) * R + r;
+        if (h->prec == TSP_PREC_FP64) reinterpret_cast<double*>(host.data())[o] = v;
+        else if (h->prec == TSP_PREC_FP32) reinterpret_cast<float*>(host.data())[o] = float(v);
+        else reinterpret_cast<__nv_bfloat16*>(host.data())[o] = __float2bfloat16_rn(float(v) / sc);
+      }
+  }
+  {
+    unsigned char* d = nullptr;
+    if ((rc = upload(h, &d, host.data(), host.size()))) return create_error_from(h, rc);
+    h->d_blocks = d;
+  }
+  if (h->prec == TSP_PREC_BF16 && (rc = upload(h, &h->d_bscale, scales.data(), scales.size())))
+    return create_error_from(h, rc);
+  if ((rc = finish_create(h))) return create_error_from(h, rc);
+  *out = h;
+  return TSP_OK;
+}
+
+int tsp_destroy(tsp_handle* h) {
+  if (!h) return TSP_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  clear_graphs(h);
+  for (void* p : h->owned) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return TSP_OK;
+}
+
+int tsp_get_sizes(const tsp_handle* h, int32_t* ne, int32_t* Np, int32_t* nshots, int32_t* nrcv, int64_t* nnzb) {
+  if (!h) return TSP_ERR_ARG;
+  if (ne) *ne = h->ne;
+  if (Np) *Np = h->Np;
+  if (nshots) *nshots = h->S;
+  if (nrcv) *nrcv = h->nrcv;
+  if (nnzb) *nnzb = h->nnzb;
+  return TSP_OK;
+}
+
+int tsp_set_dt(tsp_handle* h, double dt) {
+  if (!h) return TSP_ERR_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(h, TSP_ERR_ARG, "dt must be positive and finite");
+  h->dt = dt;
+  h->dt_set = true;
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+int tsp_force_times(double dt, int64_t n, double* out) {
+  if (n < 0 || (n > 0 && !out)) return TSP_ERR_ARG;
+  tsp::force_times(dt, n, out);
+  return TSP_OK;
+}
+
+int tsp_set_force_table(tsp_handle* h, int32_t shot, const double* F, int64_t n) {
+  if (!h) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S || n < 0 || (n > 0 && !F)) return fail(h, TSP_ERR_ARG, "bad force table");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  if (n > h->nF) {
+    // Grow the [S][nF][2] table, keeping the other shots' entries.
+    std::vector<double> grown(size_t(h->S) * n * 2, 0.0);
+    for (int s = 0; s < h->S; ++s)
+      if (h->nF)
+        std::memcpy(&grown[size_t(s) * n * 2], &h->Fhost[size_t(s) * h->nF * 2], size_t(h->nF) * 2 * sizeof(double));
+    h->Fhost.swap(grown);
+    h->nF = n;
+  }
+  std::fill(h->Fhost.begin() + size_t(shot) * h->nF * 2, h->Fhost.begin() + size_t(shot + 1) * h->nF * 2, 0.0);
+  std::memcpy(&h->Fhost[size_t(shot) * h->nF * 2], F, size_t(n) * 2 * sizeof(double));
+  // Re-upload the whole table (setup-time call).
+  if (h->d_F) {
+    TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+    dfree(h, h->d_F);
+    h->d_F = nullptr;
+  }
+  if ((rc = upload(h, &h->d_F, h->Fhost.data(), h->Fhost.size()))) return rc;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+int tsp_set_ricker(tsp_handle* h, int32_t shot, double f0, double t0, double amp, int32_t direction, int64_t n) {
+  if (!h) return TSP_ERR_ARG;
+  if (!h->dt_set) return fail(h, TSP_ERR_STATE, "tsp_set_ricker needs tsp_set_dt first");
+  if (direction != 0 && direction != 1) return fail(h, TSP_ERR_ARG, "direction must be 0 or 1");
+  if (n < 0) return fail(h, TSP_ERR_ARG, "negative length");
+  std::vector<double> t(static_cast<size_t>(n)), F(static_cast<size_t>(n) * 2, 0.0);
+  tsp::force_times(h->dt, n, t.data());
+  for (int64_t k = 0; k < n; ++k) F[size_t(k) * 2 + direction] = tsp::ricker(t[k], f0, t0, amp);
+  return tsp_set_force_table(h, shot, F.data(), n);
+}
+
+int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double* v0) {
+  if (!h) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<double> all(nstate);
+  // Level u^0 lives in d_U[0] before first_step.
+  h->cur = 0;
+  TSP_CUDA(h, cudaMemcpy(all.data(), h->d_U[0], nstate * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<double> zero(size_t(2) * h->ne * h->Np, 0.0);
+  ref_to_dev(h, shot, u0 ? u0 : zero.data(), all.data());
+  TSP_CUDA(h, cudaMemcpy(h->d_U[0], all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  if (v0 || h->d_v0) {
+    if (!h->d_v0) {
+      if ((rc = dalloc(h, &h->d_v0, nstate))) return rc;
+      TSP_CUDA(h, cudaMemset(h->d_v0, 0, nstate * sizeof(double)));
+    }
+    TSP_CUDA(h, cudaMemcpy(all.data(), h->d_v0, nstate * sizeof(double), cudaMemcpyDeviceToHost));
+    ref_to_dev(h, shot, v0 ? v0 : zero.data(), all.data());
+    TSP_CUDA(h, cudaMemcpy(h->d_v0, all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  h->steps_done = 0;
+  h->last_time = 0.0;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+int tsp_first_step(tsp_handle* h) {
+  if (!h) return TSP_ERR_ARG;
+  if (!h->dt_set) return fail(h, TSP_ERR_STATE, "first_step needs dt (tsp_set_dt)");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  if (h->steps_done != 0) {
+    // The reference only warns here (TimeAdvance.cpp:26-27); restart from u^0 is not possible.
+    return fail(h, TSP_ERR_STATE, "first_step after other steps");
+  }
+  if (h->energy_on) TSP_CUDA(h, cudaMemsetAsync(h->d_energy, 0, size_t(h->energy_cap) * sizeof(double), h->stream));
+  // u^0 is in d_U[0]; write u^1 into d_U[1].
+  if ((rc = launch_step(h, tsp::kModeFirst, h->d_U[0], h->d_v0, h->d_U[1], 0, 1.0, h->stream))) return rc;
+  tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, 1);
+  TSP_CUDA(h, cudaGetLastError());
+  h->cur = 1;
+  h->steps_done = 1;
+  h->last_time = h->dt;  // TimeAdvance.cpp:31
+  return TSP_OK;
+}
+
+int tsp_step(tsp_handle* h) {
+  if (!h) return TSP_ERR_ARG;
+  if (h->steps_done < 1) return fail(h, TSP_ERR_STATE, "step before first_step");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  double* x = h->d_U[h->cur];
+  double* prev = h->d_U[1 - h->cur];
+  if ((rc = launch_step(h, tsp::kModeStep, x, prev, prev, 0, 1.0, h->stream))) return rc;
+  tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, 1);
+  TSP_CUDA(h, cudaGetLastError());
+  h->cur = 1 - h->cur;
+  h->steps_done += 1;
+  h->last_time = h->last_time + h->dt;  // TimeAdvance.cpp:46, 230
+  return TSP_OK;
+}
+
+int tsp_run(tsp_handle* h, int64_t nsteps) {
+  if (!h) return TSP_ERR_ARG;
+  if (nsteps < 0) return fail(h, TSP_ERR_ARG, "negative step count");
+  if (nsteps == 0) return TSP_OK;
+  if (h->steps_done < 1) return fail(h, TSP_ERR_STATE, "run before first_step");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const auto key = std::make_pair((long long)nsteps, h->cur);
+  auto it = h->graphs.find(key);
+  if (it == h->graphs.end()) {
+    cudaGraph_t graph;
+    TSP_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int c = h->cur;
+    int lrc = TSP_OK;
+    for (int64_t i = 0; i < nsteps && lrc == TSP_OK; ++i) {
+      lrc = launch_step(h, tsp::kModeStep, h->d_U[c], h->d_U[1 - c], h->d_U[1 - c], int(i), 1.0, h->stream);
+      c = 1 - c;
+    }
+    tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, nsteps);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    if (lrc) return lrc;
+    if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    cudaGraphExec_t exec;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    it = h->graphs.emplace(key, exec).first;
+  }
+  TSP_CUDA(h, cudaGraphLaunch(it->second, h->stream));
+  if (nsteps & 1) h->cur = 1 - h->cur;
+  h->steps_done += nsteps;
+  for (int64_t i = 0; i < nsteps; ++i) h->last_time = h->last_time + h->dt;
+  return TSP_OK;
+}
+
+int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
+  if (!h || !ms) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  cudaEvent_t a, b;
+  TSP_CUDA(h, cudaEventCreate(&a));
+  TSP_CUDA(h, cudaEventCreate(&b));
+  TSP_CUDA(h, cudaEventRecord(a, h->stream));
+  rc = tsp_run(h, nsteps);
+  if (rc == TSP_OK) {
+    float f = 0.0f;
+    cudaError_t e = cudaEventRecord(b, h->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
+    if (e != cudaSuccess) rc = fail(h, TSP_ERR_CUDA, std::string("timing events: ") + cudaGetErrorString(e));
+    *ms = f;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time) {
+  if (!h) return TSP_ERR_ARG;
+  if (steps_done) *steps_done = h->steps_done;
+  if (last_time) *last_time = h->last_time;
+  return TSP_OK;
+}
+
+int tsp_get_u(tsp_handle* h, int32_t shot, double* out) {
+  if (!h || !out) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  std::vector<double> all(nstate);
+  TSP_CUDA(h, cudaMemcpyAsync(all.data(), h->d_U[h->cur], nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  dev_to_ref(h, shot, all.data(), out);
+  return TSP_OK;
+}
+
+int tsp_set_seismogram_capacity(tsp_handle* h, int64_t nsteps) {
+  if (!h) return TSP_ERR_ARG;
+  if (nsteps < 1) return fail(h, TSP_ERR_ARG, "capacity must be >= 1");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((rc = alloc_seis(h, nsteps))) return rc;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TSP_OK;
+}
+
+int tsp_get_seismograms(tsp_handle* h, int64_t k0, int64_t nk, double* out) {
+  if (!h) return TSP_ERR_ARG;
+  if (k0 < 0 || nk < 0 || (nk > 0 && !out)) return fail(h, TSP_ERR_ARG, "bad range");
+  if (nk > h->seis_cap) return fail(h, TSP_ERR_ARG, "range longer than the seismogram capacity");
+  if (h->nrcv == 0 || nk == 0) return TSP_OK;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t per = size_t(h->nrcv) * 2;
+  for (int s = 0; s < h->S; ++s)
+    for (int64_t k = 0; k < nk;) {
+      // Contiguous run inside the ring buffer.
+      const long long slot = (k0 + k) % h->seis_cap;
+      const long long run = std::min<long long>(nk - k, h->seis_cap - slot);
+      TSP_CUDA(h, cudaMemcpyAsync(out + (size_t(s) * nk + k) * per, h->d_seis + (size_t(s) * h->seis_cap + slot) * per,
+                                  size_t(run) * per * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      k += run;
+    }
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TSP_OK;
+}
+
+int tsp_enable_energy(tsp_handle* h, int32_t on) {
+  if (!h) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  if (on && !h->d_energy) {
+    h->energy_cap = std::max<long long>(h->seis_cap, 4096);
+    if ((rc = dalloc(h, &h->d_energy, size_t(h->energy_cap)))) return rc;
+    TSP_CUDA(h, cudaMemsetAsync(h->d_energy, 0, size_t(h->energy_cap) * sizeof(double), h->stream));
+  }
+  h->energy_on = on != 0;
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+int tsp_get_energy(tsp_handle* h, int64_t k0, int64_t nk, double* out) {
+  if (!h) return TSP_ERR_ARG;
+  if (!h->d_energy) return fail(h, TSP_ERR_STATE, "energy monitor not enabled");
+  if (k0 < 0 || nk < 0 || nk > h->energy_cap || (nk > 0 && !out)) return fail(h, TSP_ERR_ARG, "bad range");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  for (int64_t k = 0; k < nk;) {
+    const long long slot = (k0 + k) % h->energy_cap;
+    const long long run = std::min<long long>(nk - k, h->energy_cap - slot);
+    TSP_CUDA(h, cudaMemcpyAsync(out + k, h->d_energy + slot, size_t(run) * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream));
+    k += run;
+  }
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TSP_OK;
+}
+
+int tsp_get_state(tsp_handle* h, double* u_prev, double* u_cur, int64_t* steps_done, double* last_time) {
+  if (!h) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R, nref = size_t(2) * h->ne * h->Np;
+  std::vector<double> all(nstate);
+  for (int lvl = 0; lvl < 2; ++lvl) {
+    double* dst = lvl == 0 ? u_prev : u_cur;
+    if (!dst) continue;
+    const double* src = lvl == 0 ? h->d_U[1 - h->cur] : h->d_U[h->cur];
+    TSP_CUDA(h, cudaMemcpyAsync(all.data(), src, nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < h->S; ++s) dev_to_ref(h, s, all.data(), dst + size_t(s) * nref);
+  }
+  if (steps_done) *steps_done = h->steps_done;
+  if (last_time) *last_time = h->last_time;
+  return TSP_OK;
+}
+
+int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int64_t steps_done, double last_time) {
+  if (!h || !u_prev || !u_cur) return TSP_ERR_ARG;
+  if (steps_done < 1) return fail(h, TSP_ERR_ARG, "a resumable state has at least one step done");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R, nref = size_t(2) * h->ne * h->Np;
+  std::vector<double> all(nstate);
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->cur = 1;
+  for (int lvl = 0; lvl < 2; ++lvl) {
+    const double* src = lvl == 0 ? u_prev : u_cur;
+    for (int s = 0; s < h->S; ++s) ref_to_dev(h, s, src + size_t(s) * nref, all.data());
+    TSP_CUDA(h, cudaMemcpy(lvl == 0 ? h->d_U[0] : h->d_U[1], all.data(), nstate * sizeof(double),
+                           cudaMemcpyHostToDevice));
+  }
+  h->steps_done = steps_done;
+  h->last_time = last_time;
+  long long sd = steps_done;
+  TSP_CUDA(h, cudaMemcpy(h->d_step, &sd, sizeof(sd), cudaMemcpyHostToDevice));
+  clear_graphs(h);
+  return TSP_OK;
+}
+
+int tsp_check_finite(tsp_handle* h, int32_t* bad) {
+  if (!h || !bad) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  std::vector<double> all(nstate);
+  TSP_CUDA(h, cudaMemcpyAsync(all.data(), h->d_U[h->cur], nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  *bad = 0;
+  for (double v : all)
+    if (!std::isfinite(v)) {
+      *bad = 1;
+      break;
+    }
+  return TSP_OK;
+}
+
+int tsp_apply(tsp_handle* h, const double* x, double* y) {
+  if (!h || !x || !y) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  double *dx = nullptr, *dy = nullptr;
+  if ((rc = dalloc(h, &dx, nstate)) || (rc = dalloc(h, &dy, nstate))) return rc;
+  std::vector<double> all(nstate, 0.0);
+  ref_to_dev(h, 0, x, all.data());
+  TSP_CUDA(h, cudaMemcpy(dx, all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  if ((rc = launch_step(h, tsp::kModeApply, dx, nullptr, dy, 0, 1.0, h->stream))) return rc;
+  TSP_CUDA(h, cudaGetLastError());
+  TSP_CUDA(h, cudaMemcpyAsync(all.data(), dy, nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  dev_to_ref(h, 0, all.data(), y);
+  dfree(h, dx);
+  dfree(h, dy);
+  return TSP_OK;
+}
+
+int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax) {
+  if (!h || !lmax || iters < 1) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  double *da = nullptr, *db = nullptr;
+  if ((rc = dalloc(h, &da, nstate)) || (rc = dalloc(h, &db, nstate))) return rc;
+  // Deterministic start vector with all modes excited.
+  std::vector<double> x0(nstate);
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  for (size_t i = 0; i < nstate; ++i) {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    x0[i] = double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  }
+  TSP_CUDA(h, cudaMemcpy(da, x0.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  double scale = 1.0, lam = 0.0;
+  double acc[3];
+  for (int it = 0; it < iters; ++it) {
+    TSP_CUDA(h, cudaMemsetAsync(h->d_acc, 0, 3 * sizeof(double), h->stream));
+    if ((rc = launch_step(h, tsp::kModePower, da, nullptr, db, 0, scale, h->stream))) return rc;
+    TSP_CUDA(h, cudaMemcpyAsync(acc, h->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
+    TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+    lam = acc[0] / acc[1];  // Rayleigh quotient x^T B x / x^T M x
+    scale = acc[2] > 0 ? 1.0 / std::sqrt(acc[2]) : 1.0;
+    std::swap(da, db);
+  }
+  *lmax = lam;
+  dfree(h, da);
+  dfree(h, db);
+  return TSP_OK;
+}
+
+int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* blocks, double* minv) {
+  if (!h) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (row_ptr) TSP_CUDA(h, cudaMemcpy(row_ptr, h->d_row_ptr, (size_t(h->ne) + 1) * 4, cudaMemcpyDeviceToHost));
+  if (col) TSP_CUDA(h, cudaMemcpy(col, h->d_col, size_t(h->nnzb) * 4, cudaMemcpyDeviceToHost));
+  if (minv) TSP_CUDA(h, cudaMemcpy(minv, h->d_minv, size_t(h->ne) * 8, cudaMemcpyDeviceToHost));
+  if (blocks) {
+    const size_t RR = size_t(h->R) * h->R;
+    const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
+    std::vector<unsigned char> raw(size_t(h->nnzb) * RR * esz);
+    std::vector<float> sc;
+    TSP_CUDA(h, cudaMemcpy(raw.data(), h->d_blocks, raw.size(), cudaMemcpyDeviceToHost));
+    if (h->prec == TSP_PREC_BF16) {
+      sc.resize(size_t(h->nnzb));
+      TSP_CUDA(h, cudaMemcpy(sc.data(), h->d_bscale, sc.size() * 4, cudaMemcpyDeviceToHost));
+    }
+    for (long long b = 0; b < h->nnzb; ++b)
+      for (int c = 0; c < h->R; ++c)
+        for (int r = 0; r < h->R; ++r) {
+          const size_t i = size_t(b) * RR + size_t(c) * h->R + r;
+          double v;
+          if (h->prec == TSP_PREC_FP64) v = reinterpret_cast<double*>(raw.data())[i];
+          else if (h->prec == TSP_PREC_FP32) v = reinterpret_cast<float*>(raw.data())[i];
+          else v = double(__bfloat162float(reinterpret_cast<__nv_bfloat16*>(raw.data())[i])) * sc[b];
+          blocks[size_t(b) * RR + size_t(r) * h->R + c] = v;
+        }
+  }
+  return TSP_OK;
+}
+
+int tsp_export_points(tsp_handle* h, int32_t* src_elem, double* src_phi, int32_t* rcv_elem, double* rcv_phi) {
+  if (!h) return TSP_ERR_ARG;
+  if (src_elem) std::copy(h->src_elem.begin(), h->src_elem.end(), src_elem);
+  if (src_phi) std::copy(h->src_phi.begin(), h->src_phi.end(), src_phi);
+  if (rcv_elem) std::copy(h->rcv_elem.begin(), h->rcv_elem.end(), rcv_elem);
+  if (rcv_phi) std::copy(h->rcv_phi.begin(), h->rcv_phi.end(), rcv_phi);
+  return TSP_OK;
+}
+
+int tsp_gmsh_read(const char* path, int32_t* nverts, double* xy, int32_t* ne, int32_t* tri, int32_t* region) {
+  if (!path || !nverts || !ne) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  std::vector<double> vxy;
+  std::vector<int32_t> vtri, vreg;
+  std::string err;
+  if (!tsp::gmsh_read(path, &vxy, &vtri, &vreg, &err)) return fail(nullptr, TSP_ERR_MESH, err);
+  const int32_t nv = int32_t(vxy.size() / 2), nt = int32_t(vtri.size() / 3);
+  if (xy && *nverts < nv) return fail(nullptr, TSP_ERR_ARG, "xy buffer too small");
+  if (tri && *ne < nt) return fail(nullptr, TSP_ERR_ARG, "tri buffer too small");
+  *nverts = nv;
+  *ne = nt;
+  if (xy) std::copy(vxy.begin(), vxy.end(), xy);
+  if (tri) std::copy(vtri.begin(), vtri.end(), tri);
+  if (region) std::copy(vreg.begin(), vreg.end(), region);
+  return TSP_OK;
+}
+
+int tsp_mesh_neighbours(int32_t ne, const int32_t* tri, int32_t* neigh, int32_t* neighedge) {
+  if (ne <= 0 || !tri || !neigh || !neighedge) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  std::string err;
+  if (!tsp::build_neighbours(ne, tri, neigh, neighedge, &err)) return fail(nullptr, TSP_ERR_MESH, err);
+  return TSP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,375 @@
+// Host-side setup for the tspeed_b200 engine (see tsp_host.h).
+#include "tsp_host.h"
+
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <limits>
+#include <sstream>
+#include <unordered_map>
+
+namespace tsp {
+
+void gauleg(int n, double a, double b, double* x, double* w) {
+  // Newton iteration on P_n from the Chebyshev-like initial guess, one root
+  // per symmetric pair (QuadratureRule_imp.hpp:23-61).
+  const double m = (n + 1.0) / 2.0;
+  const double xm = 0.5 * (b + a), xl = 0.5 * (b - a);
+  const double eps = std::numeric_limits<double>::epsilon();
+  for (int i = 1; i <= m; ++i) {
+    double z = std::cos(M_PI * (i - 0.25) / (n + 0.5)), z1, pp;
+    do {
+      double p1 = 1.0, p2 = 0.0, p3;
+      for (int j = 1; j <= n; ++j) {
+        p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+    } while (std::abs(z - z1) > eps);
+    x[i - 1] = xm - xl * z;
+    x[n - i] = xm + xl * z;
+    w[i - 1] = 2.0 * xl / ((1.0 - z * z) * pp * pp);
+    w[n - i] = w[i - 1];
+  }
+}
+
+double jacobi(int n, int alpha, int beta, double z) {
+  if (n == 0) return 1.0;
+  const double p1_0 = 0.5 * (alpha - beta + (alpha + beta + 2.0) * z);
+  if (n == 1) return p1_0;
+  const int apb = alpha + beta;
+  double p2 = 1.0, p1 = p1_0, p = p1_0;
+  for (int k = 2; k <= n; ++k) {
+    const double a1 = 2.0 * k * (k + apb) * (2.0 * k + apb - 2.0);
+    const double a2 = (2.0 * k + apb - 1.0) * (alpha * alpha - beta * beta) / a1;
+    const double a3 = (2.0 * k + apb - 2.0) * (2.0 * k + apb - 1.0) * (2.0 * k + apb) / a1;
+    const double a4 = 2.0 * (k + alpha - 1.0) * (k + beta - 1.0) * (2.0 * k + apb) / a1;
+    p = (a2 + a3 * z) * p1 - a4 * p2;
+    p2 = p1;
+    p1 = p;
+  }
+  return p;
+}
+
+static double cij_of(int i, int j) { return std::sqrt((2.0 * i + 1) * 2.0 * (i + j + 1) / std::pow(4.0, i)); }
+
+void dubiner_phi(int N, double csi, double eta, double* phi) {
+  int s = 0;
+  const double om = 1 - eta;
+  for (int j = 0; j <= N; ++j)
+    for (int i = 0; i <= N - j; ++i, ++s) {
+      const double cij = cij_of(i, j);
+      double radial;  // (1-eta)^i P_i^{0,0}(2 csi/(1-eta) - 1)
+      if (om == 0.0) radial = (i == 0) ? 1.0 : 0.0;
+      else radial = std::pow(om, i) * jacobi(i, 0, 0, 2 * csi / om - 1);
+      phi[s] = cij * std::pow(2.0, i) * radial * jacobi(j, 2 * i + 1, 0, 2 * eta - 1);
+    }
+}
+
+void dubiner_grad(int N, double csi, double eta, double* gc, double* ge) {
+  int s = 0;
+  const double om = 1 - eta;
+  for (int j = 0; j <= N; ++j)
+    for (int i = 0; i <= N - j; ++i, ++s) {
+      const double cij = cij_of(i, j);
+      const double xx = 2 * csi / om - 1;
+      if (i == 0 && j == 0) {
+        gc[s] = 0;
+        ge[s] = 0;
+      } else if (i == 0) {
+        gc[s] = 0;
+        ge[s] = cij * (j + 2) * jacobi(j - 1, 2, 1, 2 * eta - 1);
+      } else if (j == 0) {
+        gc[s] = cij * std::pow(2.0, i) * std::pow(om, i - 1) * (i + 1) * jacobi(i - 1, 1, 1, xx);
+        ge[s] = cij * std::pow(2.0, i) *
+                (-i * std::pow(om, i - 1) * jacobi(i, 0, 0, xx) +
+                 csi * std::pow(om, i - 2) * (i + 1) * jacobi(i - 1, 1, 1, xx));
+      } else {
+        const double pj = jacobi(j, 2 * i + 1, 0, 2 * eta - 1);
+        gc[s] = cij * std::pow(2.0, i) * std::pow(om, i - 1) * (i + 1) * jacobi(i - 1, 1, 1, xx) * pj;
+        ge[s] = cij * std::pow(2.0, i) *
+                (-i * std::pow(om, i - 1) * jacobi(i, 0, 0, xx) * pj +
+                 csi * std::pow(om, i - 2) * (i + 1) * jacobi(i - 1, 1, 1, xx) * pj +
+                 std::pow(om, i) * (2 * i + j + 2) * jacobi(i, 0, 0, xx) * jacobi(j - 1, 2 * i + 2, 1, 2 * eta - 1));
+      }
+    }
+}
+
+static void edge_node(int l, double x, double* c, double* e) {
+  // QuadratureRule_imp.hpp:66-91.
+  if (l == 2) { *c = x; *e = 0.0; }
+  else if (l == 0) { *c = 1.0 - x; *e = x; }
+  else { *c = 0.0; *e = 1.0 - x; }
+}
+
+RefTables make_tables(int N) {
+  RefTables T;
+  T.N = N;
+  T.Np = np_of(N);
+  T.Q = N + 1;
+  const int Np = T.Np, Q = T.Q;
+  const size_t P2 = size_t(Np) * Np;
+  std::vector<double> x1(Q), w1(Q), x(Q), w(Q);
+  gauleg(Q, 0.0, 1.0, x1.data(), w1.data());
+  gauleg(Q, -1.0, 1.0, x.data(), w.data());
+  T.w1 = w1;
+  // Volume: collapsed Gauss rule (QuadratureRule_imp.hpp:101-113).
+  std::vector<double> gc(Np), ge(Np);
+  T.K.assign(4 * P2, 0.0);
+  for (int i = 0; i < Q; ++i)
+    for (int j = 0; j < Q; ++j) {
+      const double wq = (1 - x[i]) * w[i] * w[j] / 8.;
+      const double c = (1 + x[i]) / 2., e = (1 - x[i]) * (1 + x[j]) / 4.;
+      dubiner_grad(N, c, e, gc.data(), ge.data());
+      const double* g[2] = {gc.data(), ge.data()};
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int r = 0; r < Np; ++r)
+            for (int s = 0; s < Np; ++s) T.K[(a * 2 + b) * P2 + size_t(r) * Np + s] += wq * g[a][r] * g[b][s];
+    }
+  // Edges.
+  T.Be.assign(size_t(3) * Q * Np, 0.0);
+  T.Ge.assign(size_t(3) * 2 * Q * Np, 0.0);
+  for (int l = 0; l < 3; ++l)
+    for (int k = 0; k < Q; ++k) {
+      double c, e;
+      edge_node(l, x1[k], &c, &e);
+      dubiner_phi(N, c, e, &T.Be[(size_t(l) * Q + k) * Np]);
+      dubiner_grad(N, c, e, &T.Ge[((size_t(l) * 2 + 0) * Q + k) * Np], &T.Ge[((size_t(l) * 2 + 1) * Q + k) * Np]);
+    }
+  auto B = [&](int l, int k, int i) { return T.Be[(size_t(l) * Q + k) * Np + i]; };
+  auto G = [&](int l, int a, int k, int i) { return T.Ge[((size_t(l) * 2 + a) * Q + k) * Np + i]; };
+  T.Ws.assign(3 * P2, 0.0);
+  T.Wx.assign(9 * P2, 0.0);
+  T.Ds.assign(6 * P2, 0.0);
+  T.Dx.assign(18 * P2, 0.0);
+  for (int l = 0; l < 3; ++l)
+    for (int k = 0; k < Q; ++k) {
+      const int kk = Q - 1 - k;
+      for (int i = 0; i < Np; ++i)
+        for (int j = 0; j < Np; ++j) {
+          T.Ws[l * P2 + size_t(i) * Np + j] += w1[k] * B(l, k, i) * B(l, k, j);
+          for (int a = 0; a < 2; ++a) T.Ds[(a * 3 + l) * P2 + size_t(i) * Np + j] += w1[k] * G(l, a, k, i) * B(l, k, j);
+          for (int lp = 0; lp < 3; ++lp) {
+            T.Wx[(l * 3 + lp) * P2 + size_t(i) * Np + j] += w1[k] * B(l, k, i) * B(lp, kk, j);
+            for (int a = 0; a < 2; ++a)
+              T.Dx[((a * 3 + l) * 3 + lp) * P2 + size_t(i) * Np + j] += w1[k] * G(l, a, k, i) * B(lp, kk, j);
+          }
+        }
+    }
+  return T;
+}
+
+Geometry make_geometry(int32_t ne, const double* xy, const int32_t* tri) {
+  Geometry g;
+  g.detJ.resize(ne);
+  g.invJ.resize(size_t(ne) * 4);
+  g.elen.resize(size_t(ne) * 3);
+  g.enrm.resize(size_t(ne) * 6);
+  static const int ends[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  for (int32_t e = 0; e < ne; ++e) {
+    const double* p[3] = {xy + 2 * size_t(tri[3 * size_t(e)]), xy + 2 * size_t(tri[3 * size_t(e) + 1]),
+                          xy + 2 * size_t(tri[3 * size_t(e) + 2])};
+    // J = [p1 - p0 | p2 - p0] (Geometry.cpp:178-183), det and closed-form inverse.
+    const double j00 = p[1][0] - p[0][0], j10 = p[1][1] - p[0][1];
+    const double j01 = p[2][0] - p[0][0], j11 = p[2][1] - p[0][1];
+    const double det = j00 * j11 - j10 * j01;
+    const double invdet = 1.0 / det;
+    g.detJ[e] = det;
+    g.invJ[4 * size_t(e) + 0] = j11 * invdet;   // (0,0)
+    g.invJ[4 * size_t(e) + 1] = -j10 * invdet;  // (1,0)
+    g.invJ[4 * size_t(e) + 2] = -j01 * invdet;  // (0,1)
+    g.invJ[4 * size_t(e) + 3] = j00 * invdet;   // (1,1)
+    for (int l = 0; l < 3; ++l) {
+      const double* a = p[ends[l][0]];
+      const double* b = p[ends[l][1]];
+      const double dx = a[0] - b[0], dy = a[1] - b[1];
+      g.elen[3 * size_t(e) + l] = std::sqrt(dx * dx + dy * dy);
+      const double nx = -a[1] + b[1], ny = a[0] - b[0];
+      const double nn = std::sqrt(nx * nx + ny * ny);
+      g.enrm[6 * size_t(e) + 2 * l + 0] = nx / nn;
+      g.enrm[6 * size_t(e) + 2 * l + 1] = ny / nn;
+    }
+  }
+  return g;
+}
+
+bool build_neighbours(int32_t ne, const int32_t* tri, int32_t* neigh, int32_t* nedge, std::string* err) {
+  // Directed edge (a -> b) of face l; a neighbour owns the reversed edge.
+  static const int ends[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  std::unordered_map<uint64_t, int64_t> table;
+  table.reserve(size_t(ne) * 3 * 2);
+  auto key = [](uint32_t a, uint32_t b) { return (uint64_t(a) << 32) | b; };
+  for (int32_t e = 0; e < ne; ++e)
+    for (int l = 0; l < 3; ++l) {
+      const uint32_t a = uint32_t(tri[3 * size_t(e) + ends[l][0]]), b = uint32_t(tri[3 * size_t(e) + ends[l][1]]);
+      auto ins = table.emplace(key(a, b), int64_t(e) * 3 + l);
+      if (!ins.second) {
+        if (err) {
+          std::ostringstream os;
+          os << "directed edge (" << a << "," << b << ") shared by elements " << ins.first->second / 3 << " and " << e
+             << " (clockwise or overlapping triangles)";
+          *err = os.str();
+        }
+        return false;
+      }
+    }
+  for (int32_t e = 0; e < ne; ++e)
+    for (int l = 0; l < 3; ++l) {
+      const uint32_t a = uint32_t(tri[3 * size_t(e) + ends[l][0]]), b = uint32_t(tri[3 * size_t(e) + ends[l][1]]);
+      auto it = table.find(key(b, a));
+      if (it != table.end() && it->second / 3 != e) {
+        neigh[3 * size_t(e) + l] = int32_t(it->second / 3);
+        nedge[3 * size_t(e) + l] = int32_t(it->second % 3);
+      } else {
+        neigh[3 * size_t(e) + l] = -1;
+        nedge[3 * size_t(e) + l] = -1;
+      }
+    }
+  return true;
+}
+
+void bsr_pattern(int32_t ne, const int32_t* neigh, std::vector<int32_t>* row_ptr, std::vector<int32_t>* col,
+                 std::vector<int8_t>* bface) {
+  row_ptr->assign(size_t(ne) + 1, 0);
+  col->clear();
+  bface->clear();
+  col->reserve(size_t(ne) * 4);
+  bface->reserve(size_t(ne) * 4);
+  for (int32_t e = 0; e < ne; ++e) {
+    col->push_back(e);
+    bface->push_back(-1);
+    for (int l = 0; l < 3; ++l)
+      if (neigh[3 * size_t(e) + l] >= 0) {
+        col->push_back(neigh[3 * size_t(e) + l]);
+        bface->push_back(int8_t(l));
+      }
+    (*row_ptr)[e + 1] = int32_t(col->size());
+  }
+}
+
+int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, double px,
+                     double py, double* phi) {
+  for (int32_t e = 0; e < ne; ++e) {
+    const double* p0 = xy + 2 * size_t(tri[3 * size_t(e)]);
+    const double* p1 = xy + 2 * size_t(tri[3 * size_t(e) + 1]);
+    const double* p2 = xy + 2 * size_t(tri[3 * size_t(e) + 2]);
+    // Cheap rejection: the tolerance below is absolute and tiny, so a point
+    // far outside the bounding box can never pass.
+    const double xmin = std::fmin(p0[0], std::fmin(p1[0], p2[0])), xmax = std::fmax(p0[0], std::fmax(p1[0], p2[0]));
+    const double ymin = std::fmin(p0[1], std::fmin(p1[1], p2[1])), ymax = std::fmax(p0[1], std::fmax(p1[1], p2[1]));
+    const double pad = 1e-3 * ((xmax - xmin) + (ymax - ymin)) + 1e-6;
+    if (px < xmin - pad || px > xmax + pad || py < ymin - pad || py > ymax + pad) continue;
+    const double s = p0[1] * p2[0] - p0[0] * p2[1] + (p2[1] - p0[1]) * px + (p0[0] - p2[0]) * py;
+    const double t = p0[0] * p1[1] - p0[1] * p1[0] + (p0[1] - p1[1]) * px + (p1[0] - p0[0]) * py;
+    const double A = 1. / 2. * (-p1[1] * p2[0] + p0[1] * (-p1[0] + p2[0]) + p0[0] * (p1[1] - p2[1]) + p1[0] * p2[1]);
+    if (s > -1e-6 && t > -1e-6 && (s + t) < (2 + 1e-6) * A) {
+      const double* iJ = &g.invJ[4 * size_t(e)];
+      const double dx = px - p0[0], dy = py - p0[1];
+      const double r0 = iJ[0] * dx + iJ[2] * dy;
+      const double r1 = iJ[1] * dx + iJ[3] * dy;
+      dubiner_phi(N, r0, r1, phi);
+      return e;
+    }
+  }
+  return -1;
+}
+
+bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,
+               std::vector<int32_t>* region, std::string* err) {
+  std::ifstream f(path);
+  if (!f.is_open()) {
+    *err = "Mesh file does not exist or is corrupted: " + path;
+    return false;
+  }
+  std::string line;
+  auto skip_to = [&](const char* tag) {
+    while (std::getline(f, line))
+      if (line.find(tag) != std::string::npos) return true;
+    return false;
+  };
+  if (!skip_to("$Nodes")) {
+    *err = "cannot find $Nodes in " + path;
+    return false;
+  }
+  long nP = -1;
+  if (!(f >> nP) || nP <= 0) {
+    *err = "bad node count in " + path;
+    return false;
+  }
+  xy->assign(size_t(nP) * 2, 0.0);
+  std::unordered_map<long, int32_t> idmap;
+  idmap.reserve(size_t(nP) * 2);
+  for (long i = 0; i < nP; ++i) {
+    long id;
+    double x, y;
+    if (!(f >> id >> x >> y)) {
+      *err = "truncated $Nodes section in " + path;
+      return false;
+    }
+    f.ignore(std::numeric_limits<std::streamsize>::max(), '\n');
+    (*xy)[2 * i] = x;
+    (*xy)[2 * i + 1] = y;
+    idmap[id] = int32_t(i);
+  }
+  if (!skip_to("$Elements")) {
+    *err = "cannot find $Elements in " + path;
+    return false;
+  }
+  long nE = -1;
+  if (!(f >> nE) || nE < 0) {
+    *err = "bad element count in " + path;
+    return false;
+  }
+  tri->clear();
+  region->clear();
+  for (long i = 0; i < nE; ++i) {
+    long id, type, ntags;
+    if (!(f >> id >> type >> ntags)) {
+      *err = "truncated $Elements section in " + path;
+      return false;
+    }
+    std::vector<long> tags(size_t(ntags > 0 ? ntags : 0));
+    for (auto& t : tags) f >> t;
+    if (type == 2) {
+      long a, b, c;
+      f >> a >> b >> c;
+      auto ia = idmap.find(a), ib = idmap.find(b), ic = idmap.find(c);
+      if (ia == idmap.end() || ib == idmap.end() || ic == idmap.end()) {
+        *err = "triangle refers to an unknown node in " + path;
+        return false;
+      }
+      tri->push_back(ia->second);
+      tri->push_back(ib->second);
+      tri->push_back(ic->second);
+      region->push_back(ntags >= 2 ? int32_t(tags[1]) : 0);  // elementary tag (Mesh.cpp:231)
+    }
+    f.ignore(std::numeric_limits<std::streamsize>::max(), '\n');
+  }
+  if (tri->empty()) {
+    *err = "no triangles in " + path;
+    return false;
+  }
+  return true;
+}
+
+void force_times(double dt, int64_t n, double* out) {
+  if (n <= 0) return;
+  out[0] = 0.0;
+  double last = dt;
+  for (int64_t k = 1; k < n; ++k) {
+    const double t = last + dt;
+    out[k] = t;
+    last = t;
+  }
+}
+
+double ricker(double t, double f0, double t0, double amp) {
+  return amp * ((1 - 2 * M_PI * M_PI * (f0 * f0) * (t - t0) * (t - t0)) *
+                std::exp(-M_PI * M_PI * (f0 * f0) * (t - t0) * (t - t0)));
+}
+
+}  // namespace tsp

@@ -1,0 +1,511 @@
+// Device kernels of the tspeed_b200 engine (sm_100a).
+//
+// Data layout in HBM
+//   state   u[(e*S + s)*R + r], R = 2*Np, r = c*Np + i: element-major,
+//           shot-interleaved, FP64. One element's 2Np modes of one shot are
+//           contiguous (16-byte aligned since R is even).
+//   blocks  block-CSR of MyMat (MyMat.cpp:128-154): per element row the
+//           diagonal block first, then the face neighbours in edge order.
+//           Each 2Np x 2Np block is stored COLUMN-major (entry (r, c) at
+//           c*R + r), so the lanes of a team that own consecutive row pairs
+//           read one contiguous, coalesced run of a column.
+//   minv    1/(rho_e detJ_e) per element (Matrices_imp.hpp:187,189).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tsp {
+
+// ---------------------------------------------------------------------------
+// Shared parameter block of the step kernels.
+// ---------------------------------------------------------------------------
+enum StepMode : int {
+  kModeStep = 0,   // u^{k+1} = 2u^k - u^{k-1} + minv*(-dt*dt*(B u^k - f))     (TimeAdvance.cpp:52)
+  kModeFirst = 1,  // u^1 = u^0 + dt v^0 - minv*(dt*dt/2*(B u^0 - f))          (TimeAdvance.cpp:30)
+  kModeApply = 2,  // y = B x
+  kModePower = 3   // y = minv * (B x) with Rayleigh-quotient accumulators
+};
+
+struct StepParams {
+  int ne;
+  int S;                      // shots
+  int mode;
+  const int* row_ptr;         // [ne+1]
+  const int* col;             // [nnzb]
+  const void* blocks;         // [nnzb][R][R] column-major, BT
+  const float* bscale;        // [nnzb] (BF16 only)
+  const double* minv;         // [ne]
+  const double* x;            // u^k (gathered by neighbours)
+  const double* uprev;        // u^{k-1} (kModeStep) / v^0 or null (kModeFirst)
+  double* out;                // u^{k+1}; may alias uprev (same thread reads then writes)
+  double dt;
+  double xscale;              // kModePower: x is used as xscale*x
+  const long long* step_base; // device step counter (k = *step_base + rel)
+  int rel;
+  // sources: one point source per shot
+  const int* src_elem;        // [S]
+  const double* src_phi;      // [S][Np]
+  const double* F;            // [S][nF][2]
+  long long nF;
+  // receivers, CSR over elements
+  const int* rcv_ptr;         // [ne+1] or null
+  const int* rcv_id;          // [nrcv] receiver ids ordered by element
+  const double* rcv_phi;      // [nrcv][Np] by receiver id
+  double* seis;               // [S][cap][nrcv][2]
+  int nrcv;
+  long long seis_cap;
+  // energy monitor (null = off) and power-iteration accumulators
+  double* energy;             // [cap]
+  long long energy_cap;
+  double* acc;                // kModePower: [3]
+};
+
+// ---------------------------------------------------------------------------
+// Loads. Operator blocks are streamed once per step: ld.global.cs keeps them
+// from displacing the state in L2. The state is read through the read-only
+// path (neighbours re-read it).
+// ---------------------------------------------------------------------------
+template <typename BT>
+struct Pair;
+template <>
+struct Pair<double> {
+  static __device__ __forceinline__ void load(const double* p, double& a, double& b) {
+    const double2 v = __ldcs(reinterpret_cast<const double2*>(p));
+    a = v.x;
+    b = v.y;
+  }
+};
+template <>
+struct Pair<float> {
+  static __device__ __forceinline__ void load(const float* p, float& a, float& b) {
+    const float2 v = __ldcs(reinterpret_cast<const float2*>(p));
+    a = v.x;
+    b = v.y;
+  }
+};
+template <>
+struct Pair<__nv_bfloat16> {
+  static __device__ __forceinline__ void load(const __nv_bfloat16* p, float& a, float& b) {
+    const unsigned int v = __ldcs(reinterpret_cast<const unsigned int*>(p));
+    a = __uint_as_float(v << 16);
+    b = __uint_as_float(v & 0xffff0000u);
+  }
+};
+
+template <typename BT>
+struct AccOf { typedef float type; };
+template <>
+struct AccOf<double> { typedef double type; };
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Single-shot fused leap-frog step: block-row SpMV + inverse mass + leap-frog
+// update + source injection + receiver sampling (+ energy).
+//
+// A team of T lanes owns one element row; lane l owns row pairs
+// (2q, 2q+1), q = l + T*s. For each block column the team reads R contiguous
+// entries (one coalesced run), the column's x value is a shared-memory
+// broadcast. Small teams are packed TPW per warp.
+// ---------------------------------------------------------------------------
+template <int R, typename BT>
+struct RowTeam {
+  static constexpr int NPAIR = R / 2;
+  static constexpr int T = NPAIR <= 32 ? NPAIR : 32;
+  static constexpr int PPL = (NPAIR + T - 1) / T;
+  static constexpr int TPW = 32 / T;
+  static constexpr int WARPS = 8;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int TEAMS_PER_CTA = WARPS * TPW;
+};
+
+template <int R, typename BT>
+__global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
+  typedef RowTeam<R, BT> RT;
+  typedef typename AccOf<BT>::type AT;
+  constexpr int NP = R / 2;  // Np
+  constexpr int T = RT::T, PPL = RT::PPL, TPW = RT::TPW, NPAIR = RT::NPAIR;
+  __shared__ __align__(16) double xs[RT::WARPS][TPW][4][R];
+  __shared__ double red[RT::WARPS];
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tw = lane / T;
+  const int tl = lane - tw * T;
+  // Team g owns (element e, shot sh); the S shots of one element row are
+  // consecutive teams, so their block reads hit L2 after the first.
+  const long long g = (static_cast<long long>(blockIdx.x) * RT::WARPS + warp) * TPW + tw;
+  const int S = p.S;
+  const int e = static_cast<int>(g / S);
+  const int sh = static_cast<int>(g - static_cast<long long>(e) * S);
+  const bool active = (tw < TPW) && (e < p.ne);
+  const size_t me = (static_cast<size_t>(e) * S + sh) * R;  // this team's state offset
+
+  int rb = 0, nb = 0;
+  double (*xt)[R] = xs[warp][tw < TPW ? tw : 0];
+  if (active) {
+    rb = p.row_ptr[e];
+    nb = p.row_ptr[e + 1] - rb;
+    // Gather x of the row's block columns: contiguous 2Np modes per element.
+    for (int b = 0; b < nb; ++b) {
+      const int c = p.col[rb + b];
+      const double2* src = reinterpret_cast<const double2*>(p.x + (size_t(c) * S + sh) * R);
+      for (int q = tl; q < NPAIR; q += T) {
+        double2 v = __ldg(src + q);
+        if (p.mode == kModePower) { v.x *= p.xscale; v.y *= p.xscale; }
+        xt[b][2 * q] = v.x;
+        xt[b][2 * q + 1] = v.y;
+      }
+    }
+  }
+  __syncwarp();
+
+  AT acc[PPL][2];
+#pragma unroll
+  for (int s = 0; s < PPL; ++s) acc[s][0] = acc[s][1] = AT(0);
+
+  if (active) {
+    const BT* blk = reinterpret_cast<const BT*>(p.blocks) + size_t(rb) * R * R;
+    for (int b = 0; b < nb; ++b, blk += R * R) {
+      AT part[PPL][2];
+#pragma unroll
+      for (int s = 0; s < PPL; ++s) part[s][0] = part[s][1] = AT(0);
+#pragma unroll 8
+      for (int c = 0; c < R; ++c) {
+        const AT xv = AT(xt[b][c]);
+#pragma unroll
+        for (int s = 0; s < PPL; ++s) {
+          const int q = tl + T * s;
+          if (q < NPAIR) {
+            AT w0, w1;
+            Pair<BT>::load(blk + c * R + 2 * q, w0, w1);
+            part[s][0] = fma(w0, xv, part[s][0]);
+            part[s][1] = fma(w1, xv, part[s][1]);
+          }
+        }
+      }
+      if (p.bscale != nullptr) {
+        const AT sc = AT(p.bscale[rb + b]);
+#pragma unroll
+        for (int s = 0; s < PPL; ++s) {
+          acc[s][0] = fma(sc, part[s][0], acc[s][0]);
+          acc[s][1] = fma(sc, part[s][1], acc[s][1]);
+        }
+      } else {
+#pragma unroll
+        for (int s = 0; s < PPL; ++s) {
+          acc[s][0] += part[s][0];
+          acc[s][1] += part[s][1];
+        }
+      }
+    }
+  }
+
+  // ---- epilogue: inverse mass, leap-frog, source ----
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  double unew[PPL][2];
+  double en = 0.0;  // energy / Rayleigh partials
+  double en2 = 0.0, en3 = 0.0;
+  if (active) {
+    const double mi = p.minv[e];
+    const bool is_src = (p.src_elem != nullptr) && (p.src_elem[sh] == e) && (k < p.nF) &&
+                        (p.mode == kModeStep || p.mode == kModeFirst);
+    double Fk[2] = {0.0, 0.0};
+    if (is_src) {
+      Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+      Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+    }
+    const double dt = p.dt;
+#pragma unroll
+    for (int s = 0; s < PPL; ++s) {
+      const int q = tl + T * s;
+      if (q >= NPAIR) continue;
+      double y[2] = {double(acc[s][0]), double(acc[s][1])};
+      double* o = p.out + me + 2 * q;
+      double u[2] = {xt[0][2 * q], xt[0][2 * q + 1]};
+      double f[2] = {0.0, 0.0};
+      if (is_src) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = 2 * q + h;
+          const int comp = r / NP, i = r - comp * NP;
+          f[h] = Fk[comp] * p.src_phi[size_t(sh) * NP + i];
+        }
+      }
+      if (p.mode == kModeStep) {
+        const double2 up = *reinterpret_cast<const double2*>(p.uprev + me + 2 * q);
+        const double upv[2] = {up.x, up.y};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) unew[s][h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y[h] - f[h]));
+      } else if (p.mode == kModeFirst) {
+        double v0[2] = {0.0, 0.0};
+        if (p.uprev != nullptr) {
+          const double2 vv = *reinterpret_cast<const double2*>(p.uprev + me + 2 * q);
+          v0[0] = vv.x;
+          v0[1] = vv.y;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) unew[s][h] = (u[h] + dt * v0[h]) - mi * (dt * dt / 2 * (y[h] - f[h]));
+      } else if (p.mode == kModeApply) {
+        unew[s][0] = y[0];
+        unew[s][1] = y[1];
+      } else {  // kModePower
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          unew[s][h] = mi * y[h];
+          en += u[h] * y[h];
+          en2 += u[h] * u[h] / mi;
+          en3 += unew[s][h] * unew[s][h];
+        }
+      }
+      *reinterpret_cast<double2*>(o) = make_double2(unew[s][0], unew[s][1]);
+      if (p.energy != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double d = unew[s][h] - u[h];
+          en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * unew[s][h] * y[h];
+        }
+      }
+    }
+  }
+
+  // ---- receivers: sample the new level of this element ----
+  if (p.rcv_ptr != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
+    __syncwarp();
+    int r0 = 0, r1 = 0;
+    if (active) {
+      r0 = p.rcv_ptr[e];
+      r1 = p.rcv_ptr[e + 1];
+      if (r1 > r0) {
+#pragma unroll
+        for (int s = 0; s < PPL; ++s) {
+          const int q = tl + T * s;
+          if (q < NPAIR) {
+            xt[1][2 * q] = unew[s][0];
+            xt[1][2 * q + 1] = unew[s][1];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (active && r1 > r0) {
+      const long long slot = k % p.seis_cap;
+      for (int t = tl; t < 2 * (r1 - r0); t += T) {
+        const int rid = p.rcv_id[r0 + t / 2];
+        const int comp = t & 1;
+        const double* ph = p.rcv_phi + size_t(rid) * NP;
+        double v = 0.0;
+        for (int i = 0; i < NP; ++i) v += ph[i] * xt[1][comp * NP + i];
+        p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + comp] = v;
+      }
+    }
+  }
+
+  // ---- block reductions (energy, power iteration) ----
+  if (p.mode == kModePower || p.energy != nullptr) {
+    const int nred = (p.mode == kModePower) ? 3 : 1;
+    for (int w = 0; w < nred; ++w) {
+      double v = warp_sum(w == 0 ? en : (w == 1 ? en2 : en3));
+      __syncthreads();
+      if (lane == 0) red[warp] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < RT::WARPS; ++i) t += red[i];
+        if (p.mode == kModePower) atomicAdd(p.acc + w, t);
+        else atomicAdd(p.energy + (k % p.energy_cap), t);
+      }
+    }
+  }
+}
+
+__global__ void k_advance(long long* step, long long n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *step += n;
+}
+
+// ---------------------------------------------------------------------------
+// Operator assembly on the device from the factorised reference tables.
+//
+// For block b of row e and column c (entries r = m*Np+i, c' = n*Np+j):
+//   diagonal (c == e):
+//     |detJ| sum_ab alpha^{mn}_ab K^{ab}_ij                                   (A)
+//     + sum_faces [ pen*N^2 c_mn(face) Ws_l[i][j]                            (S)
+//                   - L/2 sum_a (beta^{mn}_a Ds^a_l[i][j] + beta^{nm}_a Ds^a_l[j][i]) ]   (I + I^T)
+//   off-diagonal (c = neighbour across face l of e, l' its face):
+//     - pen*N^2 c_mn Wx_{ll'}[i][j]
+//     + L/2 sum_a beta^{mn}_a(e,l) Dx^a_{ll'}[i][j] + L'/2 sum_a beta^{nm}_a(c,l') Dx^a_{l'l}[j][i]
+// with
+//   alpha^{mn}_ab = sum_kl C^{mn}_kl invJ[a][k] invJ[b][l]   (Hooke tensor of
+//     CTensorProduct/mat_dot, TimeAdvance.cpp:60-66, in stress_loc,
+//     Matrices_imp.hpp:73-94);
+//   beta^{mn}_a = sum_p tau^{mn}_p invJ[a][p], tau = traction of
+//     sigma(phi e_m) on n, row n (interelement, Matrices_imp.hpp:95-141);
+//   c_00 = (l+2m)n0^2 + 2m n1^2, c_11 = (l+2m)n1^2 + 2m n0^2, c_01 = c_10 = l n0 n1
+//     with harmonic means (stability, Matrices_imp.hpp:142-182;
+//     Parameters::avg_p, Parameters.cpp:37-45). The reference's factor
+//     h_scaled * ds = (1/L)(L w_k) is applied as w_k.
+// ---------------------------------------------------------------------------
+struct AssembleParams {
+  int ne, N, Np;
+  double pen_n2;             // penalty * N * N
+  const int* row_ptr;
+  const int* col;
+  const signed char* bface;  // face of the row element for each block, -1 diagonal
+  const int* neigh;          // [ne][3]
+  const int* nedge;          // [ne][3]
+  const double* invJ;        // [ne][4] (00,10,01,11)
+  const double* detJ;        // [ne]
+  const double* elen;        // [ne][3]
+  const double* enrm;        // [ne][3][2]
+  const double* lam;         // [ne]
+  const double* mu;          // [ne]
+  const double* K;           // [4][Np][Np]
+  const double* Ws;          // [3][Np][Np]
+  const double* Wx;          // [9][Np][Np]
+  const double* Ds;          // [6][Np][Np]
+  const double* Dx;          // [18][Np][Np]
+  int prec;                  // 0 fp64, 1 fp32, 2 bf16+scale
+  void* out;                 // blocks, column-major per block
+  float* scale;              // [nnzb] (bf16)
+};
+
+__device__ __forceinline__ double harm(double a, double b) { return (a + b == 0) ? 0.0 : 2 * a * b / (a + b); }
+
+// beta^{mn}_a for element e, face l: out[(m*2+n)*2 + a]
+__device__ __forceinline__ void face_beta(const AssembleParams& p, int e, int l, double* beta) {
+  const double lam = p.lam[e], mu = p.mu[e];
+  const double n0 = p.enrm[6 * size_t(e) + 2 * l], n1 = p.enrm[6 * size_t(e) + 2 * l + 1];
+  const double* iJ = p.invJ + 4 * size_t(e);  // iJ[a + 2*k] = invJ(a, k)
+  double tau[4][2];
+  tau[0][0] = (lam + 2 * mu) * n0; tau[0][1] = mu * n1;   // (0,0)
+  tau[1][0] = lam * n1;            tau[1][1] = mu * n0;   // (0,1)
+  tau[2][0] = mu * n1;             tau[2][1] = lam * n0;  // (1,0)
+  tau[3][0] = mu * n0;             tau[3][1] = (lam + 2 * mu) * n1;  // (1,1)
+  for (int mn = 0; mn < 4; ++mn)
+    for (int a = 0; a < 2; ++a) beta[mn * 2 + a] = tau[mn][0] * iJ[a] + tau[mn][1] * iJ[a + 2];
+}
+
+__device__ __forceinline__ double block_entry(const AssembleParams& p, int e, int c, int face, int r, int cc,
+                                              const double* alpha, const double* betas /*[3][8]*/,
+                                              const double* cmn /*[3][4]*/, const double* betan /*[8]*/) {
+  const int Np = p.Np;
+  const size_t P2 = size_t(Np) * Np;
+  const int m = r / Np, i = r - m * Np, n = cc / Np, j = cc - n * Np;
+  const int mn = m * 2 + n, nm = n * 2 + m;
+  double v = 0.0;
+  if (face < 0) {
+    const double adet = fabs(p.detJ[e]);
+    double a = 0.0;
+    for (int ab = 0; ab < 4; ++ab) a += alpha[mn * 4 + ab] * p.K[ab * P2 + size_t(i) * Np + j];
+    v = adet * a;
+    for (int l = 0; l < 3; ++l) {
+      if (p.neigh[3 * size_t(e) + l] < 0) continue;
+      const double L = p.elen[3 * size_t(e) + l];
+      v += p.pen_n2 * cmn[l * 4 + mn] * p.Ws[l * P2 + size_t(i) * Np + j];
+      double t = 0.0;
+      for (int a = 0; a < 2; ++a) {
+        const double* D = p.Ds + (a * 3 + l) * P2;
+        t += betas[l * 8 + mn * 2 + a] * D[size_t(i) * Np + j] + betas[l * 8 + nm * 2 + a] * D[size_t(j) * Np + i];
+      }
+      v -= 0.5 * L * t;
+    }
+  } else {
+    const int l = face, lp = p.nedge[3 * size_t(e) + l];
+    const double L = p.elen[3 * size_t(e) + l], Lp = p.elen[3 * size_t(c) + lp];
+    v = -p.pen_n2 * cmn[l * 4 + mn] * p.Wx[(l * 3 + lp) * P2 + size_t(i) * Np + j];
+    double t1 = 0.0, t2 = 0.0;
+    for (int a = 0; a < 2; ++a) {
+      t1 += betas[l * 8 + mn * 2 + a] * p.Dx[((a * 3 + l) * 3 + lp) * P2 + size_t(i) * Np + j];
+      t2 += betan[nm * 2 + a] * p.Dx[((a * 3 + lp) * 3 + l) * P2 + size_t(j) * Np + i];
+    }
+    v += 0.5 * L * t1 + 0.5 * Lp * t2;
+  }
+  return v;
+}
+
+// One CTA per block.
+__global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
+  const int b = blockIdx.x;
+  __shared__ int s_e;
+  __shared__ double alpha[16], betas[24], cmn[12], betan[8];
+  __shared__ float s_max[8];
+  // Find the row of block b (binary search over row_ptr).
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = p.ne - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.row_ptr[mid] <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    s_e = lo;
+  }
+  __syncthreads();
+  const int e = s_e, c = p.col[b], face = p.bface[b];
+  if (threadIdx.x == 0) {
+    const double lam = p.lam[e], mu = p.mu[e];
+    const double* iJ = p.invJ + 4 * size_t(e);
+    // C^{mn}_{kl} (k,l index physical derivatives), row-major [mn][k*2+l].
+    double C[4][4] = {{lam + 2 * mu, 0, 0, mu}, {0, lam, mu, 0}, {0, mu, lam, 0}, {mu, 0, 0, lam + 2 * mu}};
+    for (int mn = 0; mn < 4; ++mn)
+      for (int a = 0; a < 2; ++a)
+        for (int bb = 0; bb < 2; ++bb) {
+          double s = 0.0;
+          for (int kk = 0; kk < 2; ++kk)
+            for (int ll = 0; ll < 2; ++ll) s += C[mn][kk * 2 + ll] * iJ[a + 2 * kk] * iJ[bb + 2 * ll];
+          alpha[mn * 4 + a * 2 + bb] = s;
+        }
+    for (int l = 0; l < 3; ++l) {
+      const int nb = p.neigh[3 * size_t(e) + l];
+      if (nb < 0) {
+        for (int q = 0; q < 8; ++q) betas[l * 8 + q] = 0.0;
+        for (int q = 0; q < 4; ++q) cmn[l * 4 + q] = 0.0;
+        continue;
+      }
+      face_beta(p, e, l, betas + l * 8);
+      const double al = harm(p.lam[e], p.lam[nb]), am = harm(p.mu[e], p.mu[nb]);
+      const double n0 = p.enrm[6 * size_t(e) + 2 * l], n1 = p.enrm[6 * size_t(e) + 2 * l + 1];
+      cmn[l * 4 + 0] = (al + 2 * am) * n0 * n0 + 2 * am * n1 * n1;
+      cmn[l * 4 + 3] = (al + 2 * am) * n1 * n1 + 2 * am * n0 * n0;
+      cmn[l * 4 + 1] = al * n0 * n1;
+      cmn[l * 4 + 2] = al * n0 * n1;
+    }
+    if (face >= 0) face_beta(p, c, p.nedge[3 * size_t(e) + face], betan);
+  }
+  __syncthreads();
+  const int R = 2 * p.Np;
+  const int RR = R * R;
+  float amax = 0.0f;
+  if (p.prec == 2) {
+    for (int t = threadIdx.x; t < RR; t += blockDim.x) {
+      const int cc = t / R, r = t - cc * R;
+      amax = fmaxf(amax, float(fabs(block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan))));
+    }
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = amax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float m = 0.0f;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
+      // Power-of-two scale: values land in [-1, 1] and scaling is exact.
+      const float sc = (m > 0.0f) ? exp2f(ceilf(log2f(m))) : 1.0f;
+      s_max[0] = sc;
+      p.scale[b] = sc;
+    }
+    __syncthreads();
+  }
+  const float inv_sc = (p.prec == 2) ? 1.0f / s_max[0] : 1.0f;
+  for (int t = threadIdx.x; t < RR; t += blockDim.x) {
+    const int cc = t / R, r = t - cc * R;  // column-major storage: t = cc*R + r
+    const double v = block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan);
+    const size_t o = size_t(b) * RR + t;
+    if (p.prec == 0) reinterpret_cast<double*>(p.out)[o] = v;
+    else if (p.prec == 1) reinterpret_cast<float*>(p.out)[o] = float(v);
+    else reinterpret_cast<__nv_bfloat16*>(p.out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
+  }
+}
+
+}  // namespace tsp

@@ -141,7 +141,7 @@ def _interior_points(m: Mesh, n: int, rng, margin: float = 0.05):
 
 
 def config(k: int, scale: float = 1.0, seed: int = 1234, nshots: int | None = None,
-           nsteps: int | None = None) -> Problem:
+           nsteps: int | None = None, shot_seed: int | None = None) -> Problem:
     """The five benchmark configurations, optionally shrunk by `scale` (grid
     squares per axis scale by it; materials, degree and source types are kept).
 
@@ -178,7 +178,7 @@ def config(k: int, scale: float = 1.0, seed: int = 1234, nshots: int | None = No
         vp = 3000.0 * np.exp(rng.normal(0.0, 0.1, size=m.ne) - 0.5 * 0.1 ** 2)
         lam, mu, rho = lame(vp, vp / math.sqrt(3.0), np.full(m.ne, 2300.0))
         ns = 64 if nshots is None else nshots
-        pts = _interior_points(m, ns, rng)
+        pts = _interior_points(m, ns, rng if shot_seed is None else np.random.default_rng(shot_seed))
         f0 = 10.0
         src = [Source(x, y, f0, 1.0 / f0) for (x, y) in pts]
         return Problem("config3", m, 5, lam, mu, rho, src, surface_receivers(m, 128), nsteps or 3000, seed=seed)
