@@ -27,6 +27,7 @@ struct tsp_handle {
   int ne = 0, N = 0, Np = 0, R = 0, S = 1, nrcv = 0;
   long long nnzb = 0;
   int prec = TSP_PREC_FP64, op_kind = TSP_OP_EXPLICIT;
+  int bpitch = 0;  // column pitch of stored blocks: 2Np (one shot) or 2Np rounded up to 4 (batched)
   // operator
   int* d_row_ptr = nullptr;
   int* d_col = nullptr;
@@ -163,8 +164,34 @@ int finish_create(tsp_handle* h) {
   return TSP_OK;
 }
 
+template <int R, typename BT>
+int launch_batched(tsp_handle* h, const tsp::StepParams& p, dim3 grid, cudaStream_t st) {
+  typedef tsp::BatchCfg<R> CF;
+  typedef typename tsp::AccOf<BT>::type AT;
+  const size_t smem = CF::template smem_bytes<AT>();
+  static unsigned long long configured = 0;  // per instantiation, one bit per device
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched<R, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("batched kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  tsp::k_step_batched<R, BT><<<grid, CF::NT, smem, st>>>(p);
+  return TSP_OK;
+}
+
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
+    typedef tsp::BatchCfg<R> CF;
+    const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
+    switch (h->prec) {
+      case TSP_PREC_FP64: return launch_batched<R, double>(h, p, grid, st);
+      case TSP_PREC_FP32: return launch_batched<R, float>(h, p, grid, st);
+      default: return launch_batched<R, __nv_bfloat16>(h, p, grid, st);
+    }
+  }
   typedef tsp::RowTeam<R, double> RT;
   const long long teams = (long long)h->ne * h->S;
   const unsigned grid = unsigned((teams + RT::TEAMS_PER_CTA - 1) / RT::TEAMS_PER_CTA);
@@ -186,6 +213,7 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
   p.row_ptr = h->d_row_ptr;
   p.col = h->d_col;
   p.blocks = h->d_blocks;
+  p.bpitch = h->bpitch;
   p.bscale = (h->prec == TSP_PREC_BF16) ? h->d_bscale : nullptr;
   p.minv = h->d_minv;
   p.x = x;
@@ -222,6 +250,11 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
   }
 }
 
+// The single-shot row kernel reads columns of exactly 2Np entries; the
+// batched kernel reads four rows at a time and wants the column pitch
+// rounded up to 4 (zero padded).
+int block_pitch(int R, int S) { return S > 1 ? ((R + 3) & ~3) : R; }
+
 // Reference layout u[c*ne*Np + e*Np + i] <-> device layout [(e*S+s)*R + c*Np + i].
 void ref_to_dev(const tsp_handle* h, int shot, const double* src, double* dst_all) {
   const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
@@ -238,6 +271,36 @@ void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* ds
                   Np * sizeof(double));
 }
 
+
+// One shot's slice of a device state buffer (ne runs of R doubles with a
+// stride of S*R) to/from a reference-layout host vector (NULL: zeros).
+int get_shot(tsp_handle* h, const double* dsrc, int shot, double* out) {
+  const int ne = h->ne, R = h->R;
+  std::vector<double> slice(size_t(ne) * R);
+  TSP_CUDA(h, cudaMemcpy2DAsync(slice.data(), size_t(R) * sizeof(double), dsrc + size_t(shot) * R,
+                                size_t(h->S) * R * sizeof(double), size_t(R) * sizeof(double), ne,
+                                cudaMemcpyDeviceToHost, h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int e = 0; e < ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(out + size_t(c) * ne * h->Np + size_t(e) * h->Np, &slice[size_t(e) * R + size_t(c) * h->Np],
+                  h->Np * sizeof(double));
+  return TSP_OK;
+}
+int put_shot(tsp_handle* h, double* ddst, int shot, const double* in) {
+  const int ne = h->ne, R = h->R;
+  std::vector<double> slice(size_t(ne) * R, 0.0);
+  if (in)
+    for (int e = 0; e < ne; ++e)
+      for (int c = 0; c < 2; ++c)
+        std::memcpy(&slice[size_t(e) * R + size_t(c) * h->Np], in + size_t(c) * ne * h->Np + size_t(e) * h->Np,
+                    h->Np * sizeof(double));
+  TSP_CUDA(h, cudaMemcpy2DAsync(ddst + size_t(shot) * R, size_t(h->S) * R * sizeof(double), slice.data(),
+                                size_t(R) * sizeof(double), size_t(R) * sizeof(double), ne, cudaMemcpyHostToDevice,
+                                h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TSP_OK;
+}
 
 int begin(tsp_handle* h) {
   cudaError_t e = cudaSetDevice(h->device);
@@ -372,18 +435,20 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
       (rc = upload(h, &d_Ws, T.Ws.data(), T.Ws.size())) || (rc = upload(h, &d_Wx, T.Wx.data(), T.Wx.size())) ||
       (rc = upload(h, &d_Ds, T.Ds.data(), T.Ds.size())) || (rc = upload(h, &d_Dx, T.Dx.data(), T.Dx.size())))
     return create_error_from(h, rc);
-  const size_t RR = size_t(h->R) * h->R;
+  h->bpitch = block_pitch(h->R, h->S);
+  const size_t RRp = size_t(h->R) * h->bpitch;
   const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
   {
     void* blk = nullptr;
-    cudaError_t ce = cudaMalloc(&blk, size_t(h->nnzb) * RR * esz);
+    cudaError_t ce = cudaMalloc(&blk, size_t(h->nnzb) * RRp * esz);
     if (ce != cudaSuccess) {
-      fail(h, TSP_ERR_NOMEM, "operator blocks (" + std::to_string(size_t(h->nnzb) * RR * esz) +
+      fail(h, TSP_ERR_NOMEM, "operator blocks (" + std::to_string(size_t(h->nnzb) * RRp * esz) +
                                  " bytes) do not fit: " + cudaGetErrorString(ce));
       return create_error_from(h, TSP_ERR_NOMEM);
     }
     h->owned.push_back(blk);
     h->d_blocks = blk;
+    if (h->bpitch != h->R) TSP_CUDA(h, cudaMemsetAsync(blk, 0, size_t(h->nnzb) * RRp * esz, h->stream));
   }
   if (h->prec == TSP_PREC_BF16 && (rc = dalloc(h, &h->d_bscale, size_t(h->nnzb)))) return create_error_from(h, rc);
   tsp::AssembleParams ap;
@@ -408,6 +473,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   ap.Ds = d_Ds;
   ap.Dx = d_Dx;
   ap.prec = h->prec;
+  ap.pitch = h->bpitch;
   ap.out = h->d_blocks;
   ap.scale = h->d_bscale;
   // Large meshes exceed the 2^31-1 grid limit only beyond 2 G blocks.
@@ -474,8 +540,10 @@ int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
   // Transpose every block to column-major and convert to the storage type.
   const int R = h->R;
   const size_t RR = size_t(R) * R;
+  h->bpitch = block_pitch(R, h->S);
+  const int BP = h->bpitch;
   const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
-  std::vector<unsigned char> host(size_t(P->nnzb) * RR * esz);
+  std::vector<unsigned char> host(size_t(P->nnzb) * R * BP * esz, 0);
   std::vector<float> scales(h->prec == TSP_PREC_BF16 ? size_t(P->nnzb) : 0);
   for (int b = 0; b < P->nnzb; ++b) {
     const double* src = P->blocks + size_t(b) * RR;
@@ -489,7 +557,7 @@ int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
     for (int r = 0; r < R; ++r)
       for (int c = 0; c < R; ++c) {
         const double v = src[size_t(r) * R + c];
-        const size_t o = size_t(b) * RR + size_t(c) * R + r;
+        const size_t o = size_t(b) * R * BP + size_t(c) * BP + r;
         if (h->prec == TSP_PREC_FP64) reinterpret_cast<double*>(host.data())[o] = v;
         else if (h->prec == TSP_PREC_FP32) reinterpret_cast<float*>(host.data())[o] = float(v);
         else reinterpret_cast<__nv_bfloat16*>(host.data())[o] = __float2bfloat16_rn(float(v) / sc);
@@ -589,21 +657,15 @@ int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double*
   if ((rc = begin(h))) return rc;
   const size_t nstate = size_t(h->ne) * h->S * h->R;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  std::vector<double> all(nstate);
   // Level u^0 lives in d_U[0] before first_step.
   h->cur = 0;
-  TSP_CUDA(h, cudaMemcpy(all.data(), h->d_U[0], nstate * sizeof(double), cudaMemcpyDeviceToHost));
-  std::vector<double> zero(size_t(2) * h->ne * h->Np, 0.0);
-  ref_to_dev(h, shot, u0 ? u0 : zero.data(), all.data());
-  TSP_CUDA(h, cudaMemcpy(h->d_U[0], all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  if ((rc = put_shot(h, h->d_U[0], shot, u0))) return rc;
   if (v0 || h->d_v0) {
     if (!h->d_v0) {
       if ((rc = dalloc(h, &h->d_v0, nstate))) return rc;
       TSP_CUDA(h, cudaMemset(h->d_v0, 0, nstate * sizeof(double)));
     }
-    TSP_CUDA(h, cudaMemcpy(all.data(), h->d_v0, nstate * sizeof(double), cudaMemcpyDeviceToHost));
-    ref_to_dev(h, shot, v0 ? v0 : zero.data(), all.data());
-    TSP_CUDA(h, cudaMemcpy(h->d_v0, all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+    if ((rc = put_shot(h, h->d_v0, shot, v0))) return rc;
   }
   h->steps_done = 0;
   h->last_time = 0.0;
@@ -718,12 +780,7 @@ int tsp_get_u(tsp_handle* h, int32_t shot, double* out) {
   if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
   int rc;
   if ((rc = begin(h))) return rc;
-  const size_t nstate = size_t(h->ne) * h->S * h->R;
-  std::vector<double> all(nstate);
-  TSP_CUDA(h, cudaMemcpyAsync(all.data(), h->d_U[h->cur], nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  dev_to_ref(h, shot, all.data(), out);
-  return TSP_OK;
+  return get_shot(h, h->d_U[h->cur], shot, out);
 }
 
 int tsp_set_seismogram_capacity(tsp_handle* h, int64_t nsteps) {
@@ -912,8 +969,9 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
   if (minv) TSP_CUDA(h, cudaMemcpy(minv, h->d_minv, size_t(h->ne) * 8, cudaMemcpyDeviceToHost));
   if (blocks) {
     const size_t RR = size_t(h->R) * h->R;
+    const int BP = h->bpitch;
     const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
-    std::vector<unsigned char> raw(size_t(h->nnzb) * RR * esz);
+    std::vector<unsigned char> raw(size_t(h->nnzb) * h->R * BP * esz);
     std::vector<float> sc;
     TSP_CUDA(h, cudaMemcpy(raw.data(), h->d_blocks, raw.size(), cudaMemcpyDeviceToHost));
     if (h->prec == TSP_PREC_BF16) {
@@ -923,7 +981,7 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
     for (long long b = 0; b < h->nnzb; ++b)
       for (int c = 0; c < h->R; ++c)
         for (int r = 0; r < h->R; ++r) {
-          const size_t i = size_t(b) * RR + size_t(c) * h->R + r;
+          const size_t i = size_t(b) * h->R * BP + size_t(c) * BP + r;
           double v;
           if (h->prec == TSP_PREC_FP64) v = reinterpret_cast<double*>(raw.data())[i];
           else if (h->prec == TSP_PREC_FP32) v = reinterpret_cast<float*>(raw.data())[i];

@@ -34,7 +34,8 @@ struct StepParams {
   int mode;
   const int* row_ptr;         // [ne+1]
   const int* col;             // [nnzb]
-  const void* blocks;         // [nnzb][R][R] column-major, BT
+  const void* blocks;         // [nnzb][R][bpitch] column-major, BT
+  int bpitch;                 // column pitch of a stored block (R, or R padded to 4)
   const float* bscale;        // [nnzb] (BF16 only)
   const double* minv;         // [ne]
   const double* x;            // u^k (gathered by neighbours)
@@ -169,8 +170,9 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   for (int s = 0; s < PPL; ++s) acc[s][0] = acc[s][1] = AT(0);
 
   if (active) {
-    const BT* blk = reinterpret_cast<const BT*>(p.blocks) + size_t(rb) * R * R;
-    for (int b = 0; b < nb; ++b, blk += R * R) {
+    const int P = p.bpitch;
+    const BT* blk = reinterpret_cast<const BT*>(p.blocks) + size_t(rb) * R * P;
+    for (int b = 0; b < nb; ++b, blk += R * P) {
       AT part[PPL][2];
 #pragma unroll
       for (int s = 0; s < PPL; ++s) part[s][0] = part[s][1] = AT(0);
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
           const int q = tl + T * s;
           if (q < NPAIR) {
             AT w0, w1;
-            Pair<BT>::load(blk + c * R + 2 * q, w0, w1);
+            Pair<BT>::load(blk + c * P + 2 * q, w0, w1);
             part[s][0] = fma(w0, xv, part[s][0]);
             part[s][1] = fma(w1, xv, part[s][1]);
           }
@@ -323,6 +325,191 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched multi-shot step: per element row a (shots x 2Np) += (shots x K) .
+// (K x 2Np) GEMM over the row's blocks, K = 2Np per block, on CUDA cores in
+// the accumulation type (FP32 for FP32/BF16 blocks, FP64 for FP64 blocks),
+// followed by the same fused leap-frog / source / receiver epilogue.
+//
+// One CTA owns (element row e, 64 shots). Per block: the block (column pitch
+// RP = 2Np rounded up to 4, zero padded) and the neighbour's state X (64
+// shots x 2Np, FP64, converted once) are staged in shared memory; X is
+// stored transposed ([c][shot]) so that each thread's 4 shots and 4 rows are
+// two 16-byte shared loads per k. Thread (tx, ty) owns shots 4tx..4tx+3 and
+// rows 4ty..4ty+3: 16 FMAs per k.
+// ---------------------------------------------------------------------------
+template <int R>
+struct BatchCfg {
+  static constexpr int RP = (R + 3) & ~3;
+  static constexpr int ST = 64;       // shots per CTA
+  static constexpr int SP = ST + 4;   // pitch of a transposed X row
+  static constexpr int TY = RP / 4;
+  static constexpr int THREADS = 16 * TY;
+  static constexpr int NT = ((THREADS + 31) / 32) * 32;
+  template <typename AT>
+  static constexpr size_t smem_bytes() { return size_t(R) * (RP + SP) * sizeof(AT) + (NT / 32) * sizeof(double); }
+};
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  static __device__ __forceinline__ void ld(const float* p, float* v) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+};
+template <>
+struct Vec4<double> {
+  static __device__ __forceinline__ void ld(const double* p, double* v) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+};
+
+template <typename BT, typename AT>
+__device__ __forceinline__ AT to_acc(BT v) { return AT(v); }
+template <>
+__device__ __forceinline__ float to_acc<__nv_bfloat16, float>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <int R, typename BT>
+__global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepParams p) {
+  typedef BatchCfg<R> CF;
+  typedef typename AccOf<BT>::type AT;
+  constexpr int NP = R / 2, RP = CF::RP, ST = CF::ST, SP = CF::SP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  AT* Bs = reinterpret_cast<AT*>(smem_raw);                 // [R][RP]
+  AT* Xs = Bs + R * RP;                                      // [R][SP]
+  double* red = reinterpret_cast<double*>(Xs + R * SP);      // [NT/32]
+
+  const int e = blockIdx.x;
+  const int s0 = blockIdx.y * ST;
+  const int S = p.S;
+  const int t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;
+  const bool comp = ty < CF::TY;
+  const int rb = p.row_ptr[e];
+  const int nb = p.row_ptr[e + 1] - rb;
+  const BT* blocks = reinterpret_cast<const BT*>(p.blocks);
+
+  AT acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = AT(0);
+
+  for (int b = 0; b < nb; ++b) {
+    const int c = p.col[rb + b];
+    // Stage the block (already in the padded column-major layout).
+    const BT* gb = blocks + size_t(rb + b) * R * RP;
+    for (int i = t; i < R * RP; i += CF::NT) Bs[i] = to_acc<BT, AT>(gb[i]);
+    // Stage X^T: thread -> (shot, row pair); shots vary fastest so the
+    // transposed shared stores are conflict-free.
+    const double* gx = p.x + size_t(c) * S * R;
+    for (int i = t; i < ST * NP; i += CF::NT) {
+      const int sl = i % ST, pr = i / ST;
+      const int sh = s0 + sl;
+      double2 v = make_double2(0.0, 0.0);
+      if (sh < S) v = __ldg(reinterpret_cast<const double2*>(gx + size_t(sh) * R) + pr);
+      Xs[(2 * pr) * SP + sl] = AT(v.x);
+      Xs[(2 * pr + 1) * SP + sl] = AT(v.y);
+    }
+    __syncthreads();
+    if (comp) {
+#pragma unroll 6
+      for (int cc = 0; cc < R; ++cc) {
+        AT xv[4], bv[4];
+        Vec4<AT>::ld(&Xs[cc * SP + 4 * tx], xv);
+        Vec4<AT>::ld(&Bs[cc * RP + 4 * ty], bv);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(xv[i], bv[j], acc[i][j]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- epilogue ----
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double mi = p.minv[e];
+  const double dt = p.dt;
+  double en = 0.0;
+  if (comp) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int sh = s0 + 4 * tx + i;
+      if (sh >= S) continue;
+      const size_t me = (size_t(e) * S + sh) * R;
+      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      double Fk[2] = {0.0, 0.0};
+      if (is_src) {
+        Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+        Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+      }
+#pragma unroll
+      for (int jp = 0; jp < 2; ++jp) {
+        const int r0 = 4 * ty + 2 * jp;
+        if (r0 >= R) continue;  // rows come in pairs (R is even)
+        const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
+        // kModeStep: u^{k-1}; kModeFirst: v^0 (absent means zero).
+        const double2 up = p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
+        const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+        double un[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + h;
+          const int cmp = r / NP, ii = r - cmp * NP;
+          const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+          const double y = double(acc[i][2 * jp + h]);
+          if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+          else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+          if (p.energy != nullptr) {
+            const double d = un[h] - u[h];
+            en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+          }
+        }
+        *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+      }
+    }
+  }
+
+  // ---- receivers ----
+  if (p.rcv_ptr != nullptr) {
+    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    if (q1 > q0) {
+      __syncthreads();  // this CTA's writes of u^{k+1} are visible after the barrier
+      const long long slot = k % p.seis_cap;
+      const int nwork = (q1 - q0) * ST * 2;
+      for (int w = t; w < nwork; w += CF::NT) {
+        const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
+        const int sh = s0 + sl;
+        if (sh >= S) continue;
+        const int rid = p.rcv_id[q];
+        const double* ph = p.rcv_phi + size_t(rid) * NP;
+        const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+        double v = 0.0;
+        for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+        p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+      }
+    }
+  }
+
+  // ---- energy ----
+  if (p.energy != nullptr) {
+    const double v = warp_sum(en);
+    if ((t & 31) == 0) red[t >> 5] = v;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < CF::NT / 32; ++w) sum += red[w];
+      atomicAdd(p.energy + (k % p.energy_cap), sum);
+    }
+  }
+}
+
 __global__ void k_advance(long long* step, long long n) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *step += n;
 }
@@ -369,6 +556,7 @@ struct AssembleParams {
   const double* Ds;          // [6][Np][Np]
   const double* Dx;          // [18][Np][Np]
   int prec;                  // 0 fp64, 1 fp32, 2 bf16+scale
+  int pitch;                 // column pitch of a stored block (>= 2Np; padding pre-zeroed)
   void* out;                 // blocks, column-major per block
   float* scale;              // [nnzb] (bf16)
 };
@@ -499,9 +687,9 @@ __global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
   }
   const float inv_sc = (p.prec == 2) ? 1.0f / s_max[0] : 1.0f;
   for (int t = threadIdx.x; t < RR; t += blockDim.x) {
-    const int cc = t / R, r = t - cc * R;  // column-major storage: t = cc*R + r
+    const int cc = t / R, r = t - cc * R;  // column-major storage: (r, cc) at cc*pitch + r
     const double v = block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan);
-    const size_t o = size_t(b) * RR + t;
+    const size_t o = size_t(b) * R * p.pitch + size_t(cc) * p.pitch + r;
     if (p.prec == 0) reinterpret_cast<double*>(p.out)[o] = v;
     else if (p.prec == 1) reinterpret_cast<float*>(p.out)[o] = float(v);
     else reinterpret_cast<__nv_bfloat16*>(p.out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
