@@ -38,6 +38,8 @@ struct tsp_handle {
   double* d_U[2] = {nullptr, nullptr};
   int cur = 0;  // d_U[cur] holds u^k, d_U[1-cur] holds u^{k-1}
   double* d_v0 = nullptr;
+  float* d_X32[2] = {nullptr, nullptr};  // FP32 transposed shadows of d_U (batched FP32 kernel)
+  bool shadow = false;
   long long* d_step = nullptr;
   // sources / receivers
   int* d_src_elem = nullptr;
@@ -148,6 +150,17 @@ int finish_create(tsp_handle* h) {
     if ((rc = dalloc(h, &h->d_U[i], nstate))) return rc;
     TSP_CUDA(h, cudaMemsetAsync(h->d_U[i], 0, nstate * sizeof(double), h->stream));
   }
+  // The FP32 batched kernel (FP32 blocks, several shots, 2Np <= 72) keeps an
+  // FP32 transposed shadow of each state level.
+  h->shadow = (h->S > 1 && h->prec == TSP_PREC_FP32 && h->R <= 72);
+  if (h->shadow) {
+    const int ntile = (h->S + 63) / 64;
+    const size_t nsh = size_t(h->ne) * ntile * h->R * 64;
+    for (int i = 0; i < 2; ++i) {
+      if ((rc = dalloc(h, &h->d_X32[i], nsh))) return rc;
+      TSP_CUDA(h, cudaMemsetAsync(h->d_X32[i], 0, nsh * sizeof(float), h->stream));
+    }
+  }
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
   if ((rc = dalloc(h, &h->d_acc, 3))) return rc;
@@ -183,6 +196,21 @@ int launch_batched(tsp_handle* h, const tsp::StepParams& p, dim3 grid, cudaStrea
 
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
+    typedef tsp::Batch32Cfg<R> CF;
+    const size_t smem = CF::smem_bytes();
+    static unsigned long long configured = 0;
+    const unsigned long long bit = 1ull << (h->device & 63);
+    if (!(configured & bit)) {
+      cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(smem));
+      if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("batched32 kernel smem: ") + cudaGetErrorString(e));
+      configured |= bit;
+    }
+    const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
+    tsp::k_step_batched32<R><<<grid, CF::NT, smem, st>>>(p);
+    return TSP_OK;
+  }
   if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::BatchCfg<R> CF;
     const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
@@ -193,7 +221,7 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
     }
   }
   typedef tsp::RowTeam<R, double> RT;
-  const long long teams = (long long)h->ne * h->S;
+  const long long teams = (long long)h->ne * p.S;
   const unsigned grid = unsigned((teams + RT::TEAMS_PER_CTA - 1) / RT::TEAMS_PER_CTA);
   switch (h->prec) {
     case TSP_PREC_FP64: tsp::k_step_rows<R, double><<<grid, RT::THREADS, 0, st>>>(p); break;
@@ -237,6 +265,15 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
   p.energy = (sample && h->energy_on) ? h->d_energy : nullptr;
   p.energy_cap = h->energy_cap;
   p.acc = h->d_acc;
+  p.x32_in = nullptr;
+  p.x32_out = nullptr;
+  if (h->shadow) {
+    // The shadow pair follows the FP64 pair: x reads d_U[i] <-> d_X32[i].
+    const int ix = (x == h->d_U[0]) ? 0 : 1;
+    p.x32_in = h->d_X32[ix];
+    p.x32_out = h->d_X32[1 - ix];
+  }
+  if (mode == tsp::kModeApply || mode == tsp::kModePower) p.S = 1;  // single-vector products
   switch (h->R) {
     case 6: return launch_R<6>(h, p, st);
     case 12: return launch_R<12>(h, p, st);
@@ -248,6 +285,15 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
     case 90: return launch_R<90>(h, p, st);
     default: return fail(h, TSP_ERR_UNSUPPORTED, "no kernel for 2Np = " + std::to_string(h->R));
   }
+}
+
+// Rebuilds the FP32 shadow of state level i from its FP64 values.
+int refresh_shadow(tsp_handle* h, int i) {
+  if (!h->shadow) return TSP_OK;
+  const int ntile = (h->S + 63) / 64;
+  tsp::k_make_shadow<<<1184, 256, 0, h->stream>>>(h->d_U[i], h->d_X32[i], h->ne, h->S, h->R, ntile);
+  TSP_CUDA(h, cudaGetLastError());
+  return TSP_OK;
 }
 
 // The single-shot row kernel reads columns of exactly 2Np entries; the
@@ -686,6 +732,7 @@ int tsp_first_step(tsp_handle* h) {
   }
   if (h->energy_on) TSP_CUDA(h, cudaMemsetAsync(h->d_energy, 0, size_t(h->energy_cap) * sizeof(double), h->stream));
   // u^0 is in d_U[0]; write u^1 into d_U[1].
+  if ((rc = refresh_shadow(h, 0))) return rc;
   if ((rc = launch_step(h, tsp::kModeFirst, h->d_U[0], h->d_v0, h->d_U[1], 0, 1.0, h->stream))) return rc;
   tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, 1);
   TSP_CUDA(h, cudaGetLastError());
@@ -880,6 +927,7 @@ int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int6
     TSP_CUDA(h, cudaMemcpy(lvl == 0 ? h->d_U[0] : h->d_U[1], all.data(), nstate * sizeof(double),
                            cudaMemcpyHostToDevice));
   }
+  if ((rc = refresh_shadow(h, 1))) return rc;
   h->steps_done = steps_done;
   h->last_time = last_time;
   long long sd = steps_done;
@@ -909,17 +957,24 @@ int tsp_apply(tsp_handle* h, const double* x, double* y) {
   if (!h || !x || !y) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
-  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  // Single-vector product: temporary vectors in the one-shot layout [e][R].
+  const size_t n1 = size_t(h->ne) * h->R;
   double *dx = nullptr, *dy = nullptr;
-  if ((rc = dalloc(h, &dx, nstate)) || (rc = dalloc(h, &dy, nstate))) return rc;
-  std::vector<double> all(nstate, 0.0);
-  ref_to_dev(h, 0, x, all.data());
-  TSP_CUDA(h, cudaMemcpy(dx, all.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  if ((rc = dalloc(h, &dx, n1)) || (rc = dalloc(h, &dy, n1))) return rc;
+  std::vector<double> v(n1, 0.0);
+  for (int e = 0; e < h->ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(&v[size_t(e) * h->R + size_t(c) * h->Np], x + size_t(c) * h->ne * h->Np + size_t(e) * h->Np,
+                  h->Np * sizeof(double));
+  TSP_CUDA(h, cudaMemcpy(dx, v.data(), n1 * sizeof(double), cudaMemcpyHostToDevice));
   if ((rc = launch_step(h, tsp::kModeApply, dx, nullptr, dy, 0, 1.0, h->stream))) return rc;
   TSP_CUDA(h, cudaGetLastError());
-  TSP_CUDA(h, cudaMemcpyAsync(all.data(), dy, nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TSP_CUDA(h, cudaMemcpyAsync(v.data(), dy, n1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  dev_to_ref(h, 0, all.data(), y);
+  for (int e = 0; e < h->ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(y + size_t(c) * h->ne * h->Np + size_t(e) * h->Np, &v[size_t(e) * h->R + size_t(c) * h->Np],
+                  h->Np * sizeof(double));
   dfree(h, dx);
   dfree(h, dy);
   return TSP_OK;
@@ -929,7 +984,7 @@ int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax) {
   if (!h || !lmax || iters < 1) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
-  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  const size_t nstate = size_t(h->ne) * h->R;  // one vector, layout [e][R]
   double *da = nullptr, *db = nullptr;
   if ((rc = dalloc(h, &da, nstate)) || (rc = dalloc(h, &db, nstate))) return rc;
   // Deterministic start vector with all modes excited.

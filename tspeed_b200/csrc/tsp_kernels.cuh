@@ -61,6 +61,11 @@ struct StepParams {
   double* energy;             // [cap]
   long long energy_cap;
   double* acc;                // kModePower: [3]
+  // FP32 transposed shadow of the state for the batched FP32 kernel:
+  // x32[((e*ntile + tile)*R + c)*64 + shot_in_tile]. x32_in is read by the
+  // neighbour gathers, x32_out receives u^{k+1}.
+  const float* x32_in;
+  float* x32_out;
 };
 
 // ---------------------------------------------------------------------------
@@ -507,6 +512,200 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
       for (int w = 0; w < CF::NT / 32; ++w) sum += red[w];
       atomicAdd(p.energy + (k % p.energy_cap), sum);
     }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched FP32 step with asynchronous staging. Same GEMM as k_step_batched,
+// but the neighbours' states come from the FP32 transposed shadow written by
+// the previous step's epilogue, so the blocks and the state tiles of all the
+// row's blocks are copied global->shared with cp.async (no register staging,
+// no conversion) behind a single barrier. The epilogue writes u^{k+1} in FP64
+// and its FP32 shadow (one 16-byte store per thread and row).
+// ---------------------------------------------------------------------------
+template <int R>
+struct Batch32Cfg {
+  static constexpr int RP = (R + 3) & ~3;
+  static constexpr int ST = 64;
+  static constexpr int SP = ST + 4;
+  static constexpr int TY = RP / 4;
+  static constexpr int NT = ((16 * TY + 31) / 32) * 32;
+  static constexpr size_t smem_bytes() {
+    return size_t(4) * R * (RP + SP) * sizeof(float) + (NT / 32) * sizeof(double);
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int R>
+__global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const StepParams p) {
+  typedef Batch32Cfg<R> CF;
+  constexpr int NP = R / 2, RP = CF::RP, ST = CF::ST, SP = CF::SP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* Bs = reinterpret_cast<float*>(smem_raw);        // [4][R][RP]
+  float* Xs = Bs + 4 * R * RP;                            // [4][R][SP]
+  double* red = reinterpret_cast<double*>(Xs + 4 * R * SP);
+
+  const int e = blockIdx.x;
+  const int tile = blockIdx.y, ntile = gridDim.y;
+  const int s0 = tile * ST;
+  const int S = p.S;
+  const int t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;
+  const bool comp = ty < CF::TY;
+  const int rb = p.row_ptr[e];
+  const int nb = p.row_ptr[e + 1] - rb;
+
+  // ---- stage every block of the row and every neighbour tile ----
+  {
+    const float* gb = reinterpret_cast<const float*>(p.blocks) + size_t(rb) * R * RP;
+    const int nbc = nb * R * RP / 4;  // 16-byte chunks, blocks contiguous in HBM
+    for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
+    for (int b = 0; b < nb; ++b) {
+      const int c = p.col[rb + b];
+      const float* gx = p.x32_in + (size_t(c) * ntile + tile) * R * ST;
+      float* sx = Xs + b * R * SP;
+      for (int i = t; i < R * (ST / 4); i += CF::NT) {
+        const int row = i / (ST / 4), ch = i - row * (ST / 4);
+        cp_async16(sx + row * SP + 4 * ch, gx + row * ST + 4 * ch);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  if (comp) {
+    for (int b = 0; b < nb; ++b) {
+      const float* xb = Xs + b * R * SP + 4 * tx;
+      const float* bb = Bs + b * R * RP + 4 * ty;
+#pragma unroll 6
+      for (int cc = 0; cc < R; ++cc) {
+        const float4 xv = *reinterpret_cast<const float4*>(xb + cc * SP);
+        const float4 bv = *reinterpret_cast<const float4*>(bb + cc * RP);
+        const float xa[4] = {xv.x, xv.y, xv.z, xv.w}, ba[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(xa[i], ba[j], acc[i][j]);
+      }
+    }
+  }
+
+  // ---- epilogue: leap-frog in FP64, FP64 state + FP32 shadow out ----
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double mi = p.minv[e];
+  const double dt = p.dt;
+  double en = 0.0;
+  if (comp) {
+    float sh32[4][4];  // [row j][shot i]
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sh32[j][i] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int sh = s0 + 4 * tx + i;
+      if (sh >= S) continue;
+      const size_t me = (size_t(e) * S + sh) * R;
+      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      double Fk[2] = {0.0, 0.0};
+      if (is_src) {
+        Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+        Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+      }
+#pragma unroll
+      for (int jp = 0; jp < 2; ++jp) {
+        const int r0 = 4 * ty + 2 * jp;
+        if (r0 >= R) continue;
+        const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
+        const double2 up = p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
+        const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+        double un[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + h;
+          const int cmp = r / NP, ii = r - cmp * NP;
+          const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+          const double y = double(acc[i][2 * jp + h]);
+          if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+          else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));
+          if (p.energy != nullptr) {
+            const double d = un[h] - u[h];
+            en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+          }
+          sh32[2 * jp + h][i] = float(un[h]);
+        }
+        *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+      }
+    }
+    float* gx = p.x32_out + (size_t(e) * ntile + tile) * R * ST + 4 * tx;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = 4 * ty + j;
+      if (r < R) *reinterpret_cast<float4*>(gx + r * ST) = make_float4(sh32[j][0], sh32[j][1], sh32[j][2], sh32[j][3]);
+    }
+  }
+
+  // ---- receivers ----
+  if (p.rcv_ptr != nullptr) {
+    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    if (q1 > q0) {
+      __syncthreads();
+      const long long slot = k % p.seis_cap;
+      const int nwork = (q1 - q0) * ST * 2;
+      for (int w = t; w < nwork; w += CF::NT) {
+        const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
+        const int sh = s0 + sl;
+        if (sh >= S) continue;
+        const int rid = p.rcv_id[q];
+        const double* ph = p.rcv_phi + size_t(rid) * NP;
+        const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+        double v = 0.0;
+        for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+        p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+      }
+    }
+  }
+
+  if (p.energy != nullptr) {
+    const double v = warp_sum(en);
+    if ((t & 31) == 0) red[t >> 5] = v;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < CF::NT / 32; ++w) sum += red[w];
+      atomicAdd(p.energy + (k % p.energy_cap), sum);
+    }
+  }
+}
+
+// FP32 transposed shadow of a whole FP64 state (before first_step and after
+// tsp_set_state): one thread per (element, tile, row, shot-in-tile).
+__global__ void k_make_shadow(const double* __restrict__ u, float* __restrict__ x32, int ne, int S, int R,
+                              int ntile) {
+  const long long n = (long long)ne * ntile * R * 64;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int sl = int(i & 63);
+    long long rest = i >> 6;
+    const int r = int(rest % R);
+    rest /= R;
+    const int tile = int(rest % ntile);
+    const long long e = rest / ntile;
+    const int sh = tile * 64 + sl;
+    x32[i] = (sh < S) ? float(u[(e * S + sh) * R + r]) : 0.0f;
   }
 }
 
