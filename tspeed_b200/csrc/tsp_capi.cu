@@ -40,6 +40,8 @@ struct tsp_handle {
   double* d_v0 = nullptr;
   float* d_X32[2] = {nullptr, nullptr};  // FP32 transposed shadows of d_U (batched FP32 kernel)
   bool shadow = false;
+  bool pipelined = true;  // persistent cp.async pipeline for the FP32 batched step
+  int num_sms = 148;
   long long* d_step = nullptr;
   // sources / receivers
   int* d_src_elem = nullptr;
@@ -194,8 +196,30 @@ int launch_batched(tsp_handle* h, const tsp::StepParams& p, dim3 grid, cudaStrea
   return TSP_OK;
 }
 
+template <int R, int ST, int TR>
+int launch_pipe(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::PipeCfg<R, ST, TR> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32p<R, ST, TR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("pipelined kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  const long long items = (long long)h->ne * ((h->S + ST - 1) / ST);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched32p<R, ST, TR><<<grid, CF::NT, smem, st>>>(p);
+  return TSP_OK;
+}
+
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->pipelined) {
+    if constexpr (R <= 42) return launch_pipe<R, 64, 4>(h, p, st);
+    else if constexpr (R <= 56) return launch_pipe<R, 32, 2>(h, p, st);
+  }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::Batch32Cfg<R> CF;
     const size_t smem = CF::smem_bytes();
@@ -363,6 +387,7 @@ int make_handle(int device, tsp_handle** out) {
   tsp_handle* h = new tsp_handle();
   h->device = device;
   e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete h;

@@ -692,6 +692,237 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent, software-pipelined batched FP32 step (the production form of
+// k_step_batched32). One CTA per SM walks the work items (element row,
+// shot tile) round-robin. Per item i:
+//   - cp.async group T_i: the item's FP64 state tiles u^k and u^{k-1}
+//     (needed only by the epilogue, so their latency hides behind the GEMM);
+//   - cp.async group G_{i+1}: the next item's blocks and neighbour FP32 tiles
+//     into the other stage buffer;
+//   - wait G_i, GEMM from shared memory, wait T_i, fused epilogue.
+// Thread (tx, ty) owns shots 4tx..4tx+3 and rows TR*ty..TR*ty+TR-1.
+// ---------------------------------------------------------------------------
+template <int R, int ST, int TR>
+struct PipeCfg {
+  static constexpr int RP = (R + 3) & ~3;   // block column pitch (floats)
+  static constexpr int UP = R + 2;          // state tile pitch (doubles), breaks bank alignment
+  static constexpr int TX = ST / 4;
+  static constexpr int TY = RP / TR;
+  static constexpr int NT = ((TX * TY + 31) / 32) * 32;
+  static constexpr int STAGE = 4 * R * RP + 4 * R * ST;  // floats per stage
+  static constexpr size_t smem_bytes() {
+    return size_t(2) * STAGE * sizeof(float) + size_t(2) * ST * UP * sizeof(double) + (NT / 32) * sizeof(double);
+  }
+};
+
+template <int TR>
+struct RowVec;
+template <>
+struct RowVec<4> {
+  static __device__ __forceinline__ void ld(const float* p, float* v) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+};
+template <>
+struct RowVec<2> {
+  static __device__ __forceinline__ void ld(const float* p, float* v) {
+    const float2 a = *reinterpret_cast<const float2*>(p);
+    v[0] = a.x; v[1] = a.y;
+  }
+};
+
+template <int R, int ST, int TR>
+__global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(const StepParams p) {
+  typedef PipeCfg<R, ST, TR> CF;
+  constexpr int NP = R / 2, RP = CF::RP, UP = CF::UP, TX = CF::TX, TY = CF::TY;
+  constexpr int NTILE_SH = 64;  // shots per tile of the FP32 shadow layout
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* stage0 = reinterpret_cast<float*>(smem_raw);
+  double* Uk = reinterpret_cast<double*>(stage0 + 2 * CF::STAGE);  // [ST][UP]
+  double* Up = Uk + ST * UP;                                          // [ST][UP]
+  double* red = Up + ST * UP;
+
+  const int S = p.S;
+  const int ntile = (S + ST - 1) / ST;
+  const int nsh_tile = (S + NTILE_SH - 1) / NTILE_SH;
+  const long long nitems = (long long)p.ne * ntile;
+  const int t = threadIdx.x;
+  const int tx = t % TX, ty = t / TX;
+  const bool comp = ty < TY;
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double dt = p.dt;
+
+  // Issue the cp.async copies of an item's blocks and neighbour tiles.
+  auto issue_operands = [&](long long item, float* st) {
+    const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
+    const int s0 = tile * ST;
+    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    float* Bs = st;
+    float* Xs = st + 4 * R * RP;
+    const float* gb = reinterpret_cast<const float*>(p.blocks) + size_t(rb) * R * RP;
+    const int nbc = nb * R * RP / 4;
+    for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
+    const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
+    for (int b = 0; b < nb; ++b) {
+      const int c = p.col[rb + b];
+      const float* gx = p.x32_in + (size_t(c) * nsh_tile + sht) * R * NTILE_SH + sho;
+      float* sx = Xs + b * R * ST;
+      for (int i = t; i < R * (ST / 4); i += CF::NT) {
+        const int row = i / (ST / 4), ch = i - row * (ST / 4);
+        cp_async16(sx + row * ST + 4 * ch, gx + row * NTILE_SH + 4 * ch);
+      }
+    }
+  };
+  // Issue the cp.async copies of an item's FP64 state tiles (valid shots only).
+  auto issue_state = [&](long long item) {
+    const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
+    const int s0 = tile * ST;
+    const int nsv = min(ST, S - s0);
+    const int cpr = R / 2;  // 16-byte chunks per shot row (R doubles)
+    const double* gk = p.x + (size_t(e) * S + s0) * R;
+    const double* gp = p.uprev ? p.uprev + (size_t(e) * S + s0) * R : nullptr;
+    for (int i = t; i < nsv * cpr; i += CF::NT) {
+      const int sl = i / cpr, ch = i - sl * cpr;
+      cp_async16(Uk + sl * UP + 2 * ch, gk + size_t(sl) * R + 2 * ch);
+      if (gp) cp_async16(Up + sl * UP + 2 * ch, gp + size_t(sl) * R + 2 * ch);
+    }
+  };
+
+  long long item = blockIdx.x;
+  int buf = 0;
+  if (item < nitems) issue_operands(item, stage0);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");  // G_first
+
+  for (; item < nitems; item += gridDim.x, buf ^= 1) {
+    const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
+    const int s0 = tile * ST;
+    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    float* st = stage0 + buf * CF::STAGE;
+    issue_state(item);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");  // T_i
+    const long long nxt = item + gridDim.x;
+    if (nxt < nitems) issue_operands(nxt, stage0 + (buf ^ 1) * CF::STAGE);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");  // G_{i+1}
+    asm volatile("cp.async.wait_group 2;\n" ::: "memory");  // G_i landed
+    __syncthreads();
+
+    float acc[4][TR];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < TR; ++j) acc[i][j] = 0.0f;
+    if (comp) {
+      const float* Bs = st;
+      const float* Xs = st + 4 * R * RP;
+      for (int b = 0; b < nb; ++b) {
+        const float* xb = Xs + b * R * ST + 4 * tx;
+        const float* bb = Bs + b * R * RP + TR * ty;
+#pragma unroll 7
+        for (int cc = 0; cc < R; ++cc) {
+          const float4 xv = *reinterpret_cast<const float4*>(xb + cc * ST);
+          float bv[TR];
+          RowVec<TR>::ld(bb + cc * RP, bv);
+          const float xa[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < TR; ++j) acc[i][j] = fmaf(xa[i], bv[j], acc[i][j]);
+        }
+      }
+    }
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // T_i landed
+    __syncthreads();
+
+    // ---- epilogue ----
+    const double mi = p.minv[e];
+    double en = 0.0;
+    if (comp) {
+      float sh32[TR][4];
+#pragma unroll
+      for (int j = 0; j < TR; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) sh32[j][i] = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int sl = 4 * tx + i, sh = s0 + sl;
+        if (sh >= S) continue;
+        const size_t me = (size_t(e) * S + sh) * R;
+        const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+        double Fk[2] = {0.0, 0.0};
+        if (is_src) {
+          Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+          Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+        }
+#pragma unroll
+        for (int jp = 0; jp < TR / 2; ++jp) {
+          const int r0 = TR * ty + 2 * jp;
+          if (r0 >= R) continue;
+          const double2 uu = *reinterpret_cast<const double2*>(Uk + sl * UP + r0);
+          const double2 up = p.uprev ? *reinterpret_cast<const double2*>(Up + sl * UP + r0) : make_double2(0.0, 0.0);
+          const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+          double un[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = r0 + h;
+            const int cmp = r / NP, ii = r - cmp * NP;
+            const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+            const double y = double(acc[i][2 * jp + h]);
+            if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+            else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));
+            if (p.energy != nullptr) {
+              const double d = un[h] - u[h];
+              en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+            }
+            sh32[2 * jp + h][i] = float(un[h]);
+          }
+          *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+        }
+      }
+      const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
+      float* gx = p.x32_out + (size_t(e) * nsh_tile + sht) * R * NTILE_SH + sho + 4 * tx;
+#pragma unroll
+      for (int j = 0; j < TR; ++j) {
+        const int r = TR * ty + j;
+        if (r < R) *reinterpret_cast<float4*>(gx + r * NTILE_SH) = make_float4(sh32[j][0], sh32[j][1], sh32[j][2], sh32[j][3]);
+      }
+    }
+
+    if (p.rcv_ptr != nullptr) {
+      const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+      if (q1 > q0) {
+        __syncthreads();  // u^{k+1} of this item written by the whole CTA
+        const long long slot = k % p.seis_cap;
+        const int nwork = (q1 - q0) * ST * 2;
+        for (int w = t; w < nwork; w += CF::NT) {
+          const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
+          const int sh = s0 + sl;
+          if (sh >= S) continue;
+          const int rid = p.rcv_id[q];
+          const double* ph = p.rcv_phi + size_t(rid) * NP;
+          const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+          double v = 0.0;
+          for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+          p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+        }
+      }
+    }
+    if (p.energy != nullptr) {
+      const double v = warp_sum(en);
+      if ((t & 31) == 0) red[t >> 5] = v;
+      __syncthreads();
+      if (t == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < CF::NT / 32; ++w) sum += red[w];
+        atomicAdd(p.energy + (k % p.energy_cap), sum);
+      }
+    }
+    __syncthreads();  // stage buf and the state tiles are reused
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // FP32 transposed shadow of a whole FP64 state (before first_step and after
 // tsp_set_state): one thread per (element, tile, row, shot-in-tile).
 __global__ void k_make_shadow(const double* __restrict__ u, float* __restrict__ x32, int ne, int S, int R,
