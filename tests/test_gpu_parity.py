@@ -222,9 +222,11 @@ def test_fp32_batched_pipeline_multi_tile(N):
     rcv = W.surface_receivers(m, 6)
     n = 120
     out = {}
+    dt = None
     for prec in ("fp64", "fp32"):
         with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
-            dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
             s.set_dt(dt)
             for k in range(70):
                 s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
