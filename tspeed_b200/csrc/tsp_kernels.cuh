@@ -706,13 +706,16 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
 template <int R, int ST, int TR>
 struct PipeCfg {
   static constexpr int RP = (R + 3) & ~3;   // block column pitch (floats)
-  static constexpr int UP = R + 2;          // state tile pitch (doubles), breaks bank alignment
+  static constexpr int UP = R + 2;          // state tile pitch (doubles)
+  static constexpr int YP = R + 1;          // accumulator tile pitch (floats, odd: 2-way at most)
+  static constexpr int HP = ST + 1;         // shadow staging pitch (floats)
   static constexpr int TX = ST / 4;
   static constexpr int TY = RP / TR;
   static constexpr int NT = ((TX * TY + 31) / 32) * 32;
   static constexpr int STAGE = 4 * R * RP + 4 * R * ST;  // floats per stage
   static constexpr size_t smem_bytes() {
-    return size_t(2) * STAGE * sizeof(float) + size_t(2) * ST * UP * sizeof(double) + (NT / 32) * sizeof(double);
+    return size_t(2) * STAGE * sizeof(float) + size_t(2) * ST * UP * sizeof(double) +
+           size_t(ST) * YP * sizeof(float) + size_t(R) * HP * sizeof(float) + (NT / 32) * sizeof(double) + 16;
   }
 };
 
@@ -733,16 +736,48 @@ struct RowVec<2> {
   }
 };
 
+// GEMM of one block: acc[i][j] += X[cc][4tx+i] * B[cc][TR*ty+j] over cc, with
+// the next column's operands loaded while the current one is consumed.
+template <int R, int ST, int RP, int TR>
+__device__ __forceinline__ void block_gemm(const float* __restrict__ xb, const float* __restrict__ bb,
+                                           float (&acc)[4][TR]) {
+  float4 xv = *reinterpret_cast<const float4*>(xb);
+  float bv[TR];
+  RowVec<TR>::ld(bb, bv);
+#pragma unroll
+  for (int cc = 0; cc < R; ++cc) {
+    float4 xn = xv;
+    float bn[TR];
+#pragma unroll
+    for (int j = 0; j < TR; ++j) bn[j] = bv[j];
+    if (cc + 1 < R) {
+      xn = *reinterpret_cast<const float4*>(xb + (cc + 1) * ST);
+      RowVec<TR>::ld(bb + (cc + 1) * RP, bn);
+    }
+    const float xa[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < TR; ++j) acc[i][j] = fmaf(xa[i], bv[j], acc[i][j]);
+    xv = xn;
+#pragma unroll
+    for (int j = 0; j < TR; ++j) bv[j] = bn[j];
+  }
+}
+
 template <int R, int ST, int TR>
 __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(const StepParams p) {
   typedef PipeCfg<R, ST, TR> CF;
-  constexpr int NP = R / 2, RP = CF::RP, UP = CF::UP, TX = CF::TX, TY = CF::TY;
+  constexpr int NP = R / 2, RP = CF::RP, UP = CF::UP, YP = CF::YP, HP = CF::HP, TX = CF::TX, TY = CF::TY;
+  constexpr int NPAIR = R / 2;
   constexpr int NTILE_SH = 64;  // shots per tile of the FP32 shadow layout
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* stage0 = reinterpret_cast<float*>(smem_raw);
   double* Uk = reinterpret_cast<double*>(stage0 + 2 * CF::STAGE);  // [ST][UP]
   double* Up = Uk + ST * UP;                                          // [ST][UP]
-  double* red = Up + ST * UP;
+  float* Ys = reinterpret_cast<float*>(Up + ST * UP);                // [ST][YP]
+  float* Hs = Ys + ST * YP;                                          // [R][HP]
+  double* red = reinterpret_cast<double*>(reinterpret_cast<uintptr_t>(Hs + R * HP + 3) & ~uintptr_t(7));
 
   const int S = p.S;
   const int ntile = (S + ST - 1) / ST;
@@ -754,7 +789,6 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
   const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
   const double dt = p.dt;
 
-  // Issue the cp.async copies of an item's blocks and neighbour tiles.
   auto issue_operands = [&](long long item, float* st) {
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
@@ -775,16 +809,14 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
       }
     }
   };
-  // Issue the cp.async copies of an item's FP64 state tiles (valid shots only).
   auto issue_state = [&](long long item) {
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
     const int nsv = min(ST, S - s0);
-    const int cpr = R / 2;  // 16-byte chunks per shot row (R doubles)
     const double* gk = p.x + (size_t(e) * S + s0) * R;
     const double* gp = p.uprev ? p.uprev + (size_t(e) * S + s0) * R : nullptr;
-    for (int i = t; i < nsv * cpr; i += CF::NT) {
-      const int sl = i / cpr, ch = i - sl * cpr;
+    for (int i = t; i < nsv * NPAIR; i += CF::NT) {
+      const int sl = i / NPAIR, ch = i - sl * NPAIR;
       cp_async16(Uk + sl * UP + 2 * ch, gk + size_t(sl) * R + 2 * ch);
       if (gp) cp_async16(Up + sl * UP + 2 * ch, gp + size_t(sl) * R + 2 * ch);
     }
@@ -793,11 +825,12 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
   long long item = blockIdx.x;
   int buf = 0;
   if (item < nitems) issue_operands(item, stage0);
-  asm volatile("cp.async.commit_group;\n" ::: "memory");  // G_first
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
 
   for (; item < nitems; item += gridDim.x, buf ^= 1) {
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
+    const int nsv = min(ST, S - s0);
     const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
     float* st = stage0 + buf * CF::STAGE;
     issue_state(item);
@@ -816,95 +849,79 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
     if (comp) {
       const float* Bs = st;
       const float* Xs = st + 4 * R * RP;
-      for (int b = 0; b < nb; ++b) {
-        const float* xb = Xs + b * R * ST + 4 * tx;
-        const float* bb = Bs + b * R * RP + TR * ty;
-#pragma unroll 7
-        for (int cc = 0; cc < R; ++cc) {
-          const float4 xv = *reinterpret_cast<const float4*>(xb + cc * ST);
-          float bv[TR];
-          RowVec<TR>::ld(bb + cc * RP, bv);
-          const float xa[4] = {xv.x, xv.y, xv.z, xv.w};
+      for (int b = 0; b < nb; ++b)
+        block_gemm<R, ST, RP, TR>(Xs + b * R * ST + 4 * tx, Bs + b * R * RP + TR * ty, acc);
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < TR; ++j) acc[i][j] = fmaf(xa[i], bv[j], acc[i][j]);
-        }
-      }
+        for (int j = 0; j < TR; ++j)
+          if (TR * ty + j < R) Ys[(4 * tx + i) * YP + TR * ty + j] = acc[i][j];
     }
     asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // T_i landed
     __syncthreads();
 
-    // ---- epilogue ----
+    // ---- epilogue, row-major mapping: thread -> (shot, row pair) ----
     const double mi = p.minv[e];
     double en = 0.0;
-    if (comp) {
-      float sh32[TR][4];
+    for (int w = t; w < nsv * NPAIR; w += CF::NT) {
+      const int sl = w / NPAIR, q = w - sl * NPAIR;
+      const int sh = s0 + sl, r0 = 2 * q;
+      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const double2 uu = *reinterpret_cast<const double2*>(Uk + sl * UP + r0);
+      const double2 up = p.uprev ? *reinterpret_cast<const double2*>(Up + sl * UP + r0) : make_double2(0.0, 0.0);
+      const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+      double un[2];
 #pragma unroll
-      for (int j = 0; j < TR; ++j)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) sh32[j][i] = 0.0f;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int sl = 4 * tx + i, sh = s0 + sl;
-        if (sh >= S) continue;
-        const size_t me = (size_t(e) * S + sh) * R;
-        const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
-        double Fk[2] = {0.0, 0.0};
-        if (is_src) {
-          Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
-          Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + h;
+        const int cmp = r / NP, ii = r - cmp * NP;
+        const double f = is_src ? p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+        const double y = double(Ys[sl * YP + r]);
+        if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+        else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));
+        if (p.energy != nullptr) {
+          const double d = un[h] - u[h];
+          en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
         }
-#pragma unroll
-        for (int jp = 0; jp < TR / 2; ++jp) {
-          const int r0 = TR * ty + 2 * jp;
-          if (r0 >= R) continue;
-          const double2 uu = *reinterpret_cast<const double2*>(Uk + sl * UP + r0);
-          const double2 up = p.uprev ? *reinterpret_cast<const double2*>(Up + sl * UP + r0) : make_double2(0.0, 0.0);
-          const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
-          double un[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int r = r0 + h;
-            const int cmp = r / NP, ii = r - cmp * NP;
-            const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
-            const double y = double(acc[i][2 * jp + h]);
-            if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
-            else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));
-            if (p.energy != nullptr) {
-              const double d = un[h] - u[h];
-              en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
-            }
-            sh32[2 * jp + h][i] = float(un[h]);
-          }
-          *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
-        }
+        Hs[r * HP + sl] = float(un[h]);
       }
+      *reinterpret_cast<double2*>(p.out + (size_t(e) * S + sh) * R + r0) = make_double2(un[0], un[1]);
+    }
+    __syncthreads();
+    {
+      // FP32 shadow of u^{k+1}: rows of the 64-shot layout, 16-byte stores.
       const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
-      float* gx = p.x32_out + (size_t(e) * nsh_tile + sht) * R * NTILE_SH + sho + 4 * tx;
-#pragma unroll
-      for (int j = 0; j < TR; ++j) {
-        const int r = TR * ty + j;
-        if (r < R) *reinterpret_cast<float4*>(gx + r * NTILE_SH) = make_float4(sh32[j][0], sh32[j][1], sh32[j][2], sh32[j][3]);
+      float* gx = p.x32_out + (size_t(e) * nsh_tile + sht) * R * NTILE_SH + sho;
+      for (int w = t; w < R * (ST / 4); w += CF::NT) {
+        const int r = w / (ST / 4), c4 = w - r * (ST / 4);
+        const float* hr = Hs + r * HP + 4 * c4;
+        float4 v = make_float4(hr[0], hr[1], hr[2], hr[3]);
+        if (4 * c4 + 3 >= nsv) {  // shots past S stay zero
+          if (4 * c4 + 0 >= nsv) v.x = 0.f;
+          if (4 * c4 + 1 >= nsv) v.y = 0.f;
+          if (4 * c4 + 2 >= nsv) v.z = 0.f;
+          if (4 * c4 + 3 >= nsv) v.w = 0.f;
+        }
+        *reinterpret_cast<float4*>(gx + r * NTILE_SH + 4 * c4) = v;
       }
     }
 
     if (p.rcv_ptr != nullptr) {
       const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
       if (q1 > q0) {
-        __syncthreads();  // u^{k+1} of this item written by the whole CTA
         const long long slot = k % p.seis_cap;
         const int nwork = (q1 - q0) * ST * 2;
         for (int w = t; w < nwork; w += CF::NT) {
           const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
-          const int sh = s0 + sl;
-          if (sh >= S) continue;
+          if (sl >= nsv) continue;
           const int rid = p.rcv_id[q];
           const double* ph = p.rcv_phi + size_t(rid) * NP;
-          const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+          // u^{k+1} of this item was written to global by the whole CTA
+          // before the barrier above.
+          const double* un = p.out + (size_t(e) * S + s0 + sl) * R + cmp * NP;
           double v = 0.0;
           for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
-          p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+          p.seis[((size_t(s0 + sl) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
         }
       }
     }
@@ -918,7 +935,7 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
         atomicAdd(p.energy + (k % p.energy_cap), sum);
       }
     }
-    __syncthreads();  // stage buf and the state tiles are reused
+    __syncthreads();  // stage buf, state tiles, Ys and Hs are reused
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
