@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -41,6 +42,7 @@ struct tsp_handle {
   float* d_X32[2] = {nullptr, nullptr};  // FP32 transposed shadows of d_U (batched FP32 kernel)
   bool shadow = false;
   bool pipelined = true;  // persistent cp.async pipeline for the FP32 batched step
+  int kernel_variant = 0; // 0: K split over warp groups, 1: single-group pipeline (2Np <= 42)
   int num_sms = 148;
   long long* d_step = nullptr;
   // sources / receivers
@@ -215,10 +217,32 @@ int launch_pipe(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 template <int R>
+int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::KsplitCfg<R> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e =
+        cudaFuncSetAttribute(tsp::k_step_batched32k<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("k-split kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  const long long items = (long long)h->ne * ((h->S + CF::ST - 1) / CF::ST);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched32k<R><<<grid, CF::NT, smem, st>>>(p);
+  return TSP_OK;
+}
+
+template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->pipelined) {
-    if constexpr (R <= 42) return launch_pipe<R, 64, 4>(h, p, st);
-    else if constexpr (R <= 56) return launch_pipe<R, 32, 2>(h, p, st);
+    if constexpr (R <= 42) {
+      if (h->kernel_variant == 0) return launch_ksplit<R>(h, p, st);
+      return launch_pipe<R, 64, 4>(h, p, st);
+    } else if constexpr (R <= 56) {
+      return launch_pipe<R, 32, 2>(h, p, st);
+    }
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::Batch32Cfg<R> CF;
@@ -386,6 +410,7 @@ int make_handle(int device, tsp_handle** out) {
   if (device < 0 || device >= ndev) return fail(nullptr, TSP_ERR_ARG, "device ordinal out of range");
   tsp_handle* h = new tsp_handle();
   h->device = device;
+  if (const char* v = std::getenv("TSP_BATCHED_VARIANT")) h->kernel_variant = std::atoi(v);
   e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);

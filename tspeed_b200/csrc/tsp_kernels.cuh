@@ -940,6 +940,189 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Batched FP32 step, K split across warp groups (production kernel for
+// 2Np <= 42). Four warp groups share a persistent CTA; group g multiplies
+// block g of the current item's row (the row has at most 4 blocks), so the
+// CTA runs 4x the warps of a single-tile GEMM. Partial tiles are reduced in
+// shared memory by the epilogue. Operands for item i+1 are copied with
+// cp.async into the other stage buffer while item i is computed; the FP64
+// state is read directly by the epilogue with coalesced loads.
+// ---------------------------------------------------------------------------
+template <int R>
+struct KsplitCfg {
+  static constexpr int RP = (R + 3) & ~3;
+  static constexpr int ST = 64;
+  static constexpr int YP = R + 1;
+  static constexpr int HP = ST + 1;
+  static constexpr int TX = ST / 4;
+  static constexpr int TY = RP / 4;
+  static constexpr int GT = TX * TY;              // threads per warp group (multiple of 16)
+  static constexpr int GTW = ((GT + 31) / 32) * 32;
+  static constexpr int NT = 4 * GTW;
+  static constexpr int STAGE = 4 * R * RP + 4 * R * ST;
+  static constexpr size_t smem_bytes() {
+    return size_t(2) * STAGE * sizeof(float) + size_t(4) * ST * YP * sizeof(float) + size_t(R) * HP * sizeof(float) +
+           (NT / 32) * sizeof(double) + 16;
+  }
+};
+
+template <int R>
+__global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const StepParams p) {
+  typedef KsplitCfg<R> CF;
+  constexpr int NP = R / 2, RP = CF::RP, ST = CF::ST, YP = CF::YP, HP = CF::HP, TX = CF::TX;
+  constexpr int NPAIR = R / 2;
+  constexpr int NTILE_SH = 64;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* stage0 = reinterpret_cast<float*>(smem_raw);
+  float* Yp = stage0 + 2 * CF::STAGE;  // [4][ST][YP] partial products
+  float* Hs = Yp + 4 * ST * YP;        // [R][HP] FP32 shadow staging
+  double* red = reinterpret_cast<double*>(reinterpret_cast<uintptr_t>(Hs + R * HP + 3) & ~uintptr_t(7));
+
+  const int S = p.S;
+  const int ntile = (S + ST - 1) / ST;
+  const int nsh_tile = (S + NTILE_SH - 1) / NTILE_SH;
+  const long long nitems = (long long)p.ne * ntile;
+  const int t = threadIdx.x;
+  const int grp = t / CF::GTW, gt = t - grp * CF::GTW;
+  const int tx = gt % TX, ty = gt / TX;
+  const bool comp = gt < CF::GT;
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double dt = p.dt;
+
+  auto issue_operands = [&](long long item, float* st) {
+    const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
+    const int s0 = tile * ST;
+    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    float* Bs = st;
+    float* Xs = st + 4 * R * RP;
+    const float* gb = reinterpret_cast<const float*>(p.blocks) + size_t(rb) * R * RP;
+    const int nbc = nb * R * RP / 4;
+    for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
+    const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
+    for (int b = 0; b < nb; ++b) {
+      const int c = p.col[rb + b];
+      const float* gx = p.x32_in + (size_t(c) * nsh_tile + sht) * R * NTILE_SH + sho;
+      float* sx = Xs + b * R * ST;
+      for (int i = t; i < R * (ST / 4); i += CF::NT) {
+        const int row = i / (ST / 4), ch = i - row * (ST / 4);
+        cp_async16(sx + row * ST + 4 * ch, gx + row * NTILE_SH + 4 * ch);
+      }
+    }
+  };
+
+  long long item = blockIdx.x;
+  int buf = 0;
+  if (item < nitems) issue_operands(item, stage0);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+
+  for (; item < nitems; item += gridDim.x, buf ^= 1) {
+    const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
+    const int s0 = tile * ST;
+    const int nsv = min(ST, S - s0);
+    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    float* st = stage0 + buf * CF::STAGE;
+    const long long nxt = item + gridDim.x;
+    if (nxt < nitems) issue_operands(nxt, stage0 + (buf ^ 1) * CF::STAGE);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");  // G_{i+1}
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // G_i landed
+    __syncthreads();
+
+    if (comp && grp < nb) {
+      float acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+      block_gemm<R, ST, RP, 4>(st + 4 * R * RP + grp * R * ST + 4 * tx, st + grp * R * RP + 4 * ty, acc);
+      float* yp = Yp + grp * ST * YP;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (4 * ty + j < R) yp[(4 * tx + i) * YP + 4 * ty + j] = acc[i][j];
+    }
+    __syncthreads();
+
+    // ---- epilogue, row-major mapping: thread -> (shot, row pair) ----
+    const double mi = p.minv[e];
+    double en = 0.0;
+    for (int w = t; w < nsv * NPAIR; w += CF::NT) {
+      const int sl = w / NPAIR, q = w - sl * NPAIR;
+      const int sh = s0 + sl, r0 = 2 * q;
+      const size_t me = (size_t(e) * S + sh) * R + r0;
+      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me));
+      const double2 up = p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me) : make_double2(0.0, 0.0);
+      const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+      double un[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + h;
+        const int cmp = r / NP, ii = r - cmp * NP;
+        const double f = is_src ? p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+        float ys = 0.0f;
+        for (int g = 0; g < nb; ++g) ys += Yp[(g * ST + sl) * YP + r];
+        const double y = double(ys);
+        if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+        else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));
+        if (p.energy != nullptr) {
+          const double d = un[h] - u[h];
+          en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+        }
+        Hs[r * HP + sl] = float(un[h]);
+      }
+      *reinterpret_cast<double2*>(p.out + me) = make_double2(un[0], un[1]);
+    }
+    __syncthreads();
+    {
+      const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
+      float* gx = p.x32_out + (size_t(e) * nsh_tile + sht) * R * NTILE_SH + sho;
+      for (int w = t; w < R * (ST / 4); w += CF::NT) {
+        const int r = w / (ST / 4), c4 = w - r * (ST / 4);
+        const float* hr = Hs + r * HP + 4 * c4;
+        float4 v = make_float4(hr[0], hr[1], hr[2], hr[3]);
+        if (4 * c4 + 3 >= nsv) {
+          if (4 * c4 + 0 >= nsv) v.x = 0.f;
+          if (4 * c4 + 1 >= nsv) v.y = 0.f;
+          if (4 * c4 + 2 >= nsv) v.z = 0.f;
+          if (4 * c4 + 3 >= nsv) v.w = 0.f;
+        }
+        *reinterpret_cast<float4*>(gx + r * NTILE_SH + 4 * c4) = v;
+      }
+    }
+    if (p.rcv_ptr != nullptr) {
+      const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+      if (q1 > q0) {
+        const long long slot = k % p.seis_cap;
+        const int nwork = (q1 - q0) * ST * 2;
+        for (int w = t; w < nwork; w += CF::NT) {
+          const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
+          if (sl >= nsv) continue;
+          const int rid = p.rcv_id[q];
+          const double* ph = p.rcv_phi + size_t(rid) * NP;
+          const double* un = p.out + (size_t(e) * S + s0 + sl) * R + cmp * NP;
+          double v = 0.0;
+          for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+          p.seis[((size_t(s0 + sl) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+        }
+      }
+    }
+    if (p.energy != nullptr) {
+      const double v = warp_sum(en);
+      if ((t & 31) == 0) red[t >> 5] = v;
+      __syncthreads();
+      if (t == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < CF::NT / 32; ++w) sum += red[w];
+        atomicAdd(p.energy + (k % p.energy_cap), sum);
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // FP32 transposed shadow of a whole FP64 state (before first_step and after
 // tsp_set_state): one thread per (element, tile, row, shot-in-tile).
 __global__ void k_make_shadow(const double* __restrict__ u, float* __restrict__ x32, int ne, int S, int R,
