@@ -220,6 +220,15 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
 /* Source and receiver location: elements and basis values. */
 int tsp_export_points(tsp_handle* h, int32_t* src_elem, double* src_phi, int32_t* rcv_elem, double* rcv_phi);
 
+/* Host-side projection of initial data (FESpace::transform,
+ * FESpace_imp.hpp:136-179): the caller evaluates its field at the physical
+ * volume quadrature points (collapsed Gauss<N+1> rule, (N+1)^2 points per
+ * element) and gets the modal coefficients in the reference layout.
+ * pts/fvals are [ne][(N+1)^2][2]; out has 2*ne*Np entries. */
+int tsp_quadrature_points(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, double* pts);
+int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
+                double* out);
+
 /* Host-side mesh services (Mesh.cpp). */
 /* Gmsh 2.2 ASCII reader (Mesh::Mesh, Mesh.cpp:174-257): counts first
  * (xy/tri/region NULL), then data. region = elementary tag. */

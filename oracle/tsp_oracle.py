@@ -375,6 +375,22 @@ def assemble(sp: Space, geo: Geom, neigh, nedg, lam, mu, rho, penalty: float):
     return row_ptr, cols, blocks, minv
 
 
+def transform(sp: Space, xy, tri, geo: Geom, fun):
+    """FESpace::transform (FESpace_imp.hpp:136-179): per element
+    rhs_i = sum_q f(map(x_q)) |detJ| w_q phi_i(x_q), uh = 1/detJ * M^-1 rhs with
+    M = I for the orthonormal basis. fun(x, y) -> (fx, fy) on arrays."""
+    ne = tri.shape[0]
+    p = xy[tri]
+    n2 = sp.rule.nodes2d
+    X = p[:, 0, 0][:, None] + (p[:, 1, 0] - p[:, 0, 0])[:, None] * n2[None, :, 0] + (p[:, 2, 0] - p[:, 0, 0])[:, None] * n2[None, :, 1]
+    Y = p[:, 0, 1][:, None] + (p[:, 1, 1] - p[:, 0, 1])[:, None] * n2[None, :, 0] + (p[:, 2, 1] - p[:, 0, 1])[:, None] * n2[None, :, 1]
+    fx, fy = fun(X, Y)
+    dx = np.abs(geo.detJ)[:, None] * sp.rule.w2d[None, :]
+    rx = np.einsum("eq,qi->ei", fx * dx, sp.B)
+    ry = np.einsum("eq,qi->ei", fy * dx, sp.B)
+    return np.concatenate([(rx / geo.detJ[:, None]).ravel(), (ry / geo.detJ[:, None]).ravel()])
+
+
 # --------------------------------------------------------------------------
 # Point location, sources, receivers.
 # --------------------------------------------------------------------------

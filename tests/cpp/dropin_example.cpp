@@ -1,0 +1,73 @@
+// A simulation written the way the reference's examples are
+// (Examples/src/Wedge.cpp:20-82), with the Tspeed classes swapped for
+// tspeed_gpu. Used by tests/test_gpu_cpp_dropin.py.
+//
+// usage: dropin_example mesh.msh rcv.txt outprefix N penalty dt nsteps sx sy f0 t0 amp dir
+//                       nreg [region lambda mu rho]...
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+
+#include "tspeed_gpu.hpp"
+
+using namespace tspeed_gpu;
+
+int main(int argc, char** argv) {
+  if (argc < 15) {
+    std::fprintf(stderr, "bad arguments\n");
+    return 2;
+  }
+  int a = 1;
+  const std::string mesh = argv[a++], rcv = argv[a++], out = argv[a++];
+  const int N = std::atoi(argv[a++]);
+  const double pen = std::atof(argv[a++]), dt = std::atof(argv[a++]);
+  const int nsteps = std::atoi(argv[a++]);
+  const double sx = std::atof(argv[a++]), sy = std::atof(argv[a++]);
+  const double f0 = std::atof(argv[a++]), t0 = std::atof(argv[a++]), amp = std::atof(argv[a++]);
+  const int dir = std::atoi(argv[a++]);
+  const int nreg = std::atoi(argv[a++]);
+  try {
+    Mesh_ptr Th(new Mesh(mesh));
+    FESpace_ptr Xh(new FESpace(Th, N));
+    Parameters p(Th);
+    for (int r = 0; r < nreg; ++r) {
+      const unsigned id = unsigned(std::atoi(argv[a++]));
+      p.setp("lambda", id, std::atof(argv[a++]));
+      p.setp("mu", id, std::atof(argv[a++]));
+      p.setp("rho", id, std::atof(argv[a++]));
+    }
+    Receivers r2(Xh, rcv);
+    Force_ptr f(new PointWiseForce(
+        [=](const double& t) {
+          const double v = amp * ((1 - 2 * M_PI * M_PI * (f0 * f0) * (t - t0) * (t - t0)) *
+                                  std::exp(-M_PI * M_PI * (f0 * f0) * (t - t0) * (t - t0)));
+          return std::array<double, 2>{{dir == 0 ? v : 0.0, dir == 1 ? v : 0.0}};
+        },
+        Point(sx, sy), Xh));
+    LeapFrog TA(Xh, p, r2);
+    TA.set_dt(dt);
+    TA.set_tmax((nsteps + 0.5) * dt);
+    TA.add_force(f);
+    TA.set_penalty(pen);
+    TA.set_initial_u(Xh, [](double, double) { return std::array<double, 2>{{0, 0}}; });
+    TA.set_initial_v(Xh, [](double, double) { return std::array<double, 2>{{0, 0}}; });
+    TA.first_step();
+    TA.eval_receivers();
+    int steps = 1;
+    while (TA.is_running()) {
+      TA.step();
+      TA.eval_receivers();
+      ++steps;
+    }
+    TA.write_receivers(out);
+    const std::vector<double>& u = TA.u();
+    double s = 0;
+    for (double v : u) s += v * v;
+    std::printf("steps %d norm %.17g\n", steps, std::sqrt(s));
+  } catch (const Error& e) {
+    std::fprintf(stderr, "tspeed_gpu error %d: %s\n", e.code(), e.what());
+    return 1;
+  }
+  return 0;
+}

@@ -1,0 +1,43 @@
+"""The C++ drop-in (include/tspeed_gpu.hpp) driven like the reference's
+examples, against the reference's golden seismograms (GPU)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from helpers import rel
+from tspeed_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+pytestmark = pytest.mark.gpu
+
+
+def test_cpp_dropin_matches_reference_golden(tmp_path):
+    cxx = shutil.which("g++") or shutil.which("c++")
+    assert cxx, "no C++ compiler"
+    exe = str(tmp_path / "dropin")
+    lib = os.path.join(ROOT, "tspeed_b200")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "dropin_example.cpp"), "-L" + lib, "-ltspeed_b200",
+                    "-Wl,-rpath," + lib, "-o", exe], check=True)
+    g = load_golden("g_n2_layers")
+    m = W.Mesh(g["xy"], g["tri"], g["region"], 0.0, 0.0)
+    W.write_gmsh(str(tmp_path / "m.msh"), m)
+    W.write_rcv(str(tmp_path / "m.rcv"), g["rcv"])
+    regions = []
+    for reg in sorted(set(g["region"].tolist())):
+        e = int(np.argmax(g["region"] == reg))
+        regions += [str(reg), repr(float(g["lam"][e])), repr(float(g["mu"][e])), repr(float(g["rho"][e]))]
+    f0, t0, amp, sdir = (float(v) for v in g["ricker"])
+    args = [exe, str(tmp_path / "m.msh"), str(tmp_path / "m.rcv"), str(tmp_path / "out"), str(int(g["N"])),
+            repr(float(g["penalty"])), repr(float(g["dt"])), str(int(g["nsteps"])), repr(float(g["src"][0])),
+            repr(float(g["src"][1])), repr(f0), repr(t0), repr(amp), str(int(sdir)), str(len(regions) // 4)] + regions
+    res = subprocess.run(args, check=True, capture_output=True, text=True)
+    assert res.stdout.startswith(f"steps {int(g['nsteps'])} ")
+    seis = np.stack([np.loadtxt(str(tmp_path / f"out_rcv_{i}.out")) for i in range(len(g["rcv"]))], 1)
+    assert seis.shape == g["seis"].shape
+    ok = np.isfinite(g["seis"])
+    assert rel(seis[ok], g["seis"][ok]) < 1e-12

@@ -87,3 +87,32 @@ def test_create_validates_before_touching_a_device():
     with pytest.raises(capi.TspError) as e:
         capi.Simulation.create(m.xy, m.tri, 3, lam, mu, -rho, [(50.0, 50.0)], [])
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("N", [1, 3, 5])
+def test_projection_matches_oracle_transform(N):
+    m = W.jittered_rect(4, 3, 400.0, 300.0, seed=N)
+    pts = capi.quadrature_points(N, m.xy, m.tri)
+    fun = lambda x, y: (np.sin(x / 97.0) * np.cos(y / 61.0), 1e-3 * x * y)  # noqa: E731
+    fx, fy = fun(pts[..., 0], pts[..., 1])
+    got = capi.project(N, m.xy, m.tri, np.stack([fx, fy], -1))
+    sp = O.make_space(N)
+    tri = m.tri.astype(np.int64)
+    ref = O.transform(sp, m.xy, tri, O.geometry(m.xy, tri), fun)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+
+
+def test_projection_reproduces_polynomials_of_degree_N():
+    N = 3
+    m = W.jittered_rect(3, 2, 300.0, 200.0, seed=3)
+    pts = capi.quadrature_points(N, m.xy, m.tri)
+    f = lambda x, y: (1e-6 * x ** 3 - 2e-4 * x * y, 0.5 + 1e-5 * y ** 2)  # noqa: E731
+    fx, fy = f(pts[..., 0], pts[..., 1])
+    uh = capi.project(N, m.xy, m.tri, np.stack([fx, fy], -1))
+    # Evaluate the modal expansion back at the quadrature points.
+    sp = O.make_space(N)
+    ne, Np = m.ne, sp.Np
+    vx = uh[:ne * Np].reshape(ne, Np) @ sp.B.T
+    vy = uh[ne * Np:].reshape(ne, Np) @ sp.B.T
+    assert np.abs(vx - fx).max() < 1e-10 * max(1.0, np.abs(fx).max())
+    assert np.abs(vy - fy).max() < 1e-10 * max(1.0, np.abs(fy).max())

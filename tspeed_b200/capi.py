@@ -70,6 +70,8 @@ SIGNATURES = {
     "tsp_estimate_lmax": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "tsp_export_operator": (C.c_int, [C.c_void_p, _ip, _ip, _dp, _dp]),
     "tsp_export_points": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _dp]),
+    "tsp_quadrature_points": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp]),
+    "tsp_project": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
     "tsp_mesh_neighbours": (C.c_int, [C.c_int32, _ip, _ip, _ip]),
 }
@@ -136,6 +138,22 @@ def mesh_neighbours(tri):
     ned = np.zeros((ne, 3), dtype=np.int32)
     _check(lib().tsp_mesh_neighbours(ne, _i(tri), _i(nb), _i(ned)))
     return nb, ned
+
+
+def quadrature_points(N: int, xy, tri):
+    xy, tri = _f64(xy), _i32(tri)
+    pts = np.zeros((tri.shape[0], (N + 1) ** 2, 2))
+    _check(lib().tsp_quadrature_points(N, xy.shape[0], _d(xy), tri.shape[0], _i(tri), _d(pts)))
+    return pts
+
+
+def project(N: int, xy, tri, fvals):
+    """FESpace::transform of a field sampled at quadrature_points()."""
+    xy, tri, fvals = _f64(xy), _i32(tri), _f64(fvals)
+    Np = (N + 1) * (N + 2) // 2
+    out = np.zeros(2 * tri.shape[0] * Np)
+    _check(lib().tsp_project(N, xy.shape[0], _d(xy), tri.shape[0], _i(tri), _d(fvals), _d(out)))
+    return out
 
 
 def force_times(dt: float, n: int):

@@ -41,8 +41,10 @@ struct tsp_handle {
   double* d_v0 = nullptr;
   float* d_X32[2] = {nullptr, nullptr};  // FP32 transposed shadows of d_U (batched FP32 kernel)
   bool shadow = false;
-  bool pipelined = true;  // persistent cp.async pipeline for the FP32 batched step
-  int kernel_variant = 0; // 0: K split over warp groups, 1: single-group pipeline (2Np <= 42)
+  // FP32 batched step variant: 0 K split over warp groups (2Np <= 42) or the
+  // pipelined single group (2Np = 56); 1 pipelined single group; 2 the
+  // non-persistent cp.async kernel. Selected by TSP_BATCHED_VARIANT.
+  int kernel_variant = 0;
   int num_sms = 148;
   long long* d_step = nullptr;
   // sources / receivers
@@ -236,7 +238,7 @@ int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
-  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->pipelined) {
+  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 42) {
       if (h->kernel_variant == 0) return launch_ksplit<R>(h, p, st);
       return launch_pipe<R, 64, 4>(h, p, st);
@@ -271,10 +273,20 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::RowTeam<R, double> RT;
   const long long teams = (long long)h->ne * p.S;
   const unsigned grid = unsigned((teams + RT::TEAMS_PER_CTA - 1) / RT::TEAMS_PER_CTA);
+  const bool padded = p.bpitch != R;
   switch (h->prec) {
-    case TSP_PREC_FP64: tsp::k_step_rows<R, double><<<grid, RT::THREADS, 0, st>>>(p); break;
-    case TSP_PREC_FP32: tsp::k_step_rows<R, float><<<grid, RT::THREADS, 0, st>>>(p); break;
-    default: tsp::k_step_rows<R, __nv_bfloat16><<<grid, RT::THREADS, 0, st>>>(p); break;
+    case TSP_PREC_FP64:
+      if (padded) tsp::k_step_rows<R, double, true><<<grid, RT::THREADS, 0, st>>>(p);
+      else tsp::k_step_rows<R, double, false><<<grid, RT::THREADS, 0, st>>>(p);
+      break;
+    case TSP_PREC_FP32:
+      if (padded) tsp::k_step_rows<R, float, true><<<grid, RT::THREADS, 0, st>>>(p);
+      else tsp::k_step_rows<R, float, false><<<grid, RT::THREADS, 0, st>>>(p);
+      break;
+    default:
+      if (padded) tsp::k_step_rows<R, __nv_bfloat16, true><<<grid, RT::THREADS, 0, st>>>(p);
+      else tsp::k_step_rows<R, __nv_bfloat16, false><<<grid, RT::THREADS, 0, st>>>(p);
+      break;
   }
   return TSP_OK;
 }
@@ -1120,6 +1132,25 @@ int tsp_gmsh_read(const char* path, int32_t* nverts, double* xy, int32_t* ne, in
   if (xy) std::copy(vxy.begin(), vxy.end(), xy);
   if (tri) std::copy(vtri.begin(), vtri.end(), tri);
   if (region) std::copy(vreg.begin(), vreg.end(), region);
+  return TSP_OK;
+}
+
+int tsp_quadrature_points(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, double* pts) {
+  if (N < 1 || N > tsp::kMaxN || nverts <= 0 || ne <= 0 || !xy || !tri || !pts)
+    return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_quadrature_points");
+  for (int32_t i = 0; i < 3 * ne; ++i)
+    if (tri[i] < 0 || tri[i] >= nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  tsp::quadrature_points(N, ne, xy, tri, pts);
+  return TSP_OK;
+}
+
+int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
+                double* out) {
+  if (N < 1 || N > tsp::kMaxN || nverts <= 0 || ne <= 0 || !xy || !tri || !fvals || !out)
+    return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_project");
+  for (int32_t i = 0; i < 3 * ne; ++i)
+    if (tri[i] < 0 || tri[i] >= nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  tsp::project(N, ne, xy, tri, fvals, out);
   return TSP_OK;
 }
 

@@ -356,6 +356,65 @@ bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int
   return true;
 }
 
+static void volume_rule(int N, std::vector<double>* c, std::vector<double>* e, std::vector<double>* w) {
+  const int Q = N + 1;
+  std::vector<double> x(Q), wx(Q);
+  gauleg(Q, -1.0, 1.0, x.data(), wx.data());
+  c->resize(size_t(Q) * Q);
+  e->resize(size_t(Q) * Q);
+  w->resize(size_t(Q) * Q);
+  for (int i = 0; i < Q; ++i)
+    for (int j = 0; j < Q; ++j) {
+      (*w)[i * Q + j] = (1 - x[i]) * wx[i] * wx[j] / 8.;
+      (*c)[i * Q + j] = (1 + x[i]) / 2.;
+      (*e)[i * Q + j] = (1 - x[i]) * (1 + x[j]) / 4.;
+    }
+}
+
+void quadrature_points(int N, int32_t ne, const double* xy, const int32_t* tri, double* pts) {
+  std::vector<double> c, e, w;
+  volume_rule(N, &c, &e, &w);
+  const size_t nq = c.size();
+  for (int32_t el = 0; el < ne; ++el) {
+    const double* p0 = xy + 2 * size_t(tri[3 * size_t(el)]);
+    const double* p1 = xy + 2 * size_t(tri[3 * size_t(el) + 1]);
+    const double* p2 = xy + 2 * size_t(tri[3 * size_t(el) + 2]);
+    for (size_t q = 0; q < nq; ++q) {
+      // p0 + J x^, J = [p1 - p0 | p2 - p0]
+      pts[(size_t(el) * nq + q) * 2 + 0] = p0[0] + ((p1[0] - p0[0]) * c[q] + (p2[0] - p0[0]) * e[q]);
+      pts[(size_t(el) * nq + q) * 2 + 1] = p0[1] + ((p1[1] - p0[1]) * c[q] + (p2[1] - p0[1]) * e[q]);
+    }
+  }
+}
+
+void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out) {
+  std::vector<double> c, e, w;
+  volume_rule(N, &c, &e, &w);
+  const size_t nq = c.size();
+  const int Np = np_of(N);
+  std::vector<double> B(nq * Np);  // basis at the volume points, [q][i]
+  for (size_t q = 0; q < nq; ++q) dubiner_phi(N, c[q], e[q], &B[q * Np]);
+  const Geometry g = make_geometry(ne, xy, tri);
+  std::vector<double> rhs(2 * size_t(Np));
+  for (int32_t el = 0; el < ne; ++el) {
+    std::fill(rhs.begin(), rhs.end(), 0.0);
+    for (size_t q = 0; q < nq; ++q) {
+      const double dx = std::abs(g.detJ[el]) * w[q];  // FESpace_imp.hpp:169
+      const double* F = fvals + (size_t(el) * nq + q) * 2;
+      for (int i = 0; i < Np; ++i) {
+        rhs[i] += F[0] * dx * B[q * Np + i];
+        rhs[Np + i] += F[1] * dx * B[q * Np + i];
+      }
+    }
+    // Orthonormal basis: the reference mass is the identity (FESpace_imp.hpp:51-54),
+    // uh = 1/detJ * rhs (FESpace_imp.hpp:152-153).
+    for (int i = 0; i < Np; ++i) {
+      out[size_t(el) * Np + i] = 1. / g.detJ[el] * rhs[i];
+      out[size_t(ne) * Np + size_t(el) * Np + i] = 1. / g.detJ[el] * rhs[Np + i];
+    }
+  }
+}
+
 void force_times(double dt, int64_t n, double* out) {
   if (n <= 0) return;
   out[0] = 0.0;

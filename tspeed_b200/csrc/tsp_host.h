@@ -82,6 +82,16 @@ int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, co
 bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,
                std::vector<int32_t>* region, std::string* err);
 
+// Physical volume quadrature points of every element, [ne][Q*Q][2], in the
+// order of the collapsed Gauss<N+1> rule (QuadratureRule_imp.hpp:101-113)
+// mapped by Triangle::map (Geometry.cpp:203-207).
+void quadrature_points(int N, int32_t ne, const double* xy, const int32_t* tri, double* pts);
+
+// FESpace::transform (FESpace_imp.hpp:136-179): L2 projection of a vector
+// field given by its values at the quadrature points, fvals[ne][Q*Q][2], onto
+// the Dubiner modes, reference layout out[c*ne*Np + e*Np + i].
+void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out);
+
 // Force evaluation times (TimeAdvance.cpp:28,46 with M_last_time
 // accumulated in double, TimeAdvance.hpp:230).
 void force_times(double dt, int64_t n, double* out);

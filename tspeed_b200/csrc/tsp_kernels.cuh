@@ -130,7 +130,7 @@ struct RowTeam {
   static constexpr int TEAMS_PER_CTA = WARPS * TPW;
 };
 
-template <int R, typename BT>
+template <int R, typename BT, bool PADDED>
 __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   typedef RowTeam<R, BT> RT;
   typedef typename AccOf<BT>::type AT;
@@ -175,7 +175,9 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   for (int s = 0; s < PPL; ++s) acc[s][0] = acc[s][1] = AT(0);
 
   if (active) {
-    const int P = p.bpitch;
+    // Column pitch: 2Np for single-shot storage, rounded up to 4 when the
+    // blocks are stored for the batched kernels (compile-time either way).
+    constexpr int P = PADDED ? ((R + 3) & ~3) : R;
     const BT* blk = reinterpret_cast<const BT*>(p.blocks) + size_t(rb) * R * P;
     for (int b = 0; b < nb; ++b, blk += R * P) {
       AT part[PPL][2];
