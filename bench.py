@@ -37,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 from tspeed_b200 import capi  # noqa: E402
 from tspeed_b200 import workloads as W  # noqa: E402
+from tspeed_b200.shard import max_over_ranks, shots_for_rank  # noqa: E402
 
 METRIC = "DOF-steps/s on 1 B200: mixed/batched vs plain FP64, at seismogram err <=1e-4"
 UNIT = "DOF-steps/s"
@@ -50,6 +51,20 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def captured_traffic(kernel, ne, nshots):
+    """DRAM bytes per launch of `kernel` from the committed ncu record
+    (profiles/traffic.json), scaled to ne element rows; None if not recorded
+    for this shot count."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            rec = json.load(f)[kernel]
+    except Exception:
+        return None
+    if rec["shots"] != nshots:
+        return None
+    return rec["bytes"] * ne / rec["elements"]
 
 
 def bytes_per_step(ne, Np, nnzb, nshots, precision):
@@ -115,8 +130,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_problem(args, rank):
-    p = W.config(3, scale=args.scale, nshots=args.nshots, shot_seed=1000 + rank)
+def make_problem(args, rank, world):
+    """One global list of nshots x world shots; this rank takes its slice
+    (weak scaling: nshots per GPU)."""
+    p = W.config(3, scale=args.scale, nshots=args.nshots * world, shot_seed=1000)
+    p.sources = [p.sources[i] for i in shots_for_rank(len(p.sources), rank, world)]
     return p
 
 
@@ -223,7 +241,7 @@ def main():
                                  device_id=torch.device("cuda", local_rank))
         dist = tdist
 
-    prob = make_problem(args, rank)
+    prob = make_problem(args, rank, world)
     K, Wm = args.steps, max(3, args.warmup)
     sim = capi.Simulation.from_problem(prob, precision=args.precision, device=local_rank)
     dt, lmax = estimate_dt(sim)
@@ -242,10 +260,7 @@ def main():
     ms = sim.run_timed(K)
     clocks = sampler.stop()
     if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, device=f"cuda:{local_rank}")
         dist.barrier()
     dofs = prob.dofs_per_shot
     value = world * prob.nshots * dofs * K / (ms / 1e3)
@@ -258,7 +273,14 @@ def main():
             "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
             "config": config_dict(args, prob), "dt": dt, "lmax": lmax,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "peak_source": peak_kind,
+                         "traffic": (captured_traffic("k_step_batched32k<42>", prob.mesh.ne, prob.nshots)
+                                     if prob.nshots > 1 and args.precision == "fp32" else
+                                     captured_traffic("k_step_rows<42,double>", prob.mesh.ne, prob.nshots)
+                                     if prob.nshots == 1 and args.precision == "fp64" else None)
+                         if prob.N == 5 else None,
+                         "traffic_source": "ncu capture (profiles/traffic.json) scaled by element rows",
+                         "kernel": "k_step_batched32k<42>" if prob.nshots > 1 else "k_step_rows<42>",
+                         "peak_source": peak_kind,
                          "algorithmic_bytes_per_step": algo},
             "gpu_launches": K + 1, "clocks": clocks}
     sim.close()
