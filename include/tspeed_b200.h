@@ -213,6 +213,19 @@ int tsp_apply(tsp_handle* h, const double* x, double* y);
  * reference has no CFL estimate; dt is a user setting). dt_cfl = 2/sqrt(lmax). */
 int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax);
 
+/* Allocation-free variant of tsp_estimate_lmax. No counterpart in the
+ * reference (which has no CFL estimate). For callers that must not allocate
+ * device memory when they ask for the estimate (memory pools that forbid raw
+ * cudaMalloc, real-time loops, hosts that cap library allocations): the two
+ * iteration vectors and the accumulators live in a fixed 32 MiB file-scope
+ * device array (4 Mi doubles) that every GPU loading the library holds until
+ * exit, so 2*ne*2Np + 3 must not exceed 4,194,304 (TSP_ERR_ARG otherwise).
+ * The first call on a device looks up that array's device address; make it
+ * before any stream capture. All calls share the array: calls that overlap
+ * on the GPU (several handles, threads or streams at once) race. Calls no
+ * cudaMalloc/cudaFree. */
+int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* lmax);
+
 /* Exports of the assembled operator (explicit FP64 handles only):
  * row_ptr[ne+1], col[nnzb], blocks[nnzb][2Np][2Np] row-major, minv[ne]. */
 int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* blocks, double* minv);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "tsp_check_finite": (C.c_int, [C.c_void_p, _ip]),
     "tsp_apply": (C.c_int, [C.c_void_p, _dp, _dp]),
     "tsp_estimate_lmax": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "tsp_estimate_lmax_noalloc": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "tsp_export_operator": (C.c_int, [C.c_void_p, _ip, _ip, _dp, _dp]),
     "tsp_export_points": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _dp]),
     "tsp_quadrature_points": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp]),

@@ -361,6 +361,21 @@ int refresh_shadow(tsp_handle* h, int i) {
 // rounded up to 4 (zero padded).
 int block_pitch(int R, int S) { return S > 1 ? ((R + 3) & ~3) : R; }
 
+// Launches the step kernel family with fully prepared parameters.
+int launch_step_params(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  switch (h->R) {
+    case 6: return launch_R<6>(h, p, st);
+    case 12: return launch_R<12>(h, p, st);
+    case 20: return launch_R<20>(h, p, st);
+    case 30: return launch_R<30>(h, p, st);
+    case 42: return launch_R<42>(h, p, st);
+    case 56: return launch_R<56>(h, p, st);
+    case 72: return launch_R<72>(h, p, st);
+    case 90: return launch_R<90>(h, p, st);
+    default: return fail(h, TSP_ERR_UNSUPPORTED, "no kernel for 2Np = " + std::to_string(h->R));
+  }
+}
+
 // Reference layout u[c*ne*Np + e*Np + i] <-> device layout [(e*S+s)*R + c*Np + i].
 void ref_to_dev(const tsp_handle* h, int shot, const double* src, double* dst_all) {
   const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
@@ -1162,3 +1177,94 @@ int tsp_mesh_neighbours(int32_t ne, const int32_t* tri, int32_t* neigh, int32_t*
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free power iteration.
+//
+// For callers that may not allocate device memory at the time they need a
+// CFL estimate: code running under a caching allocator or memory pool that
+// forbids raw cudaMalloc, real-time loops where an allocation's implicit
+// synchronisation is unacceptable, or applications that own all device memory
+// and cap what libraries may take. The two iteration vectors and the three
+// accumulators live in this file-scope array instead of cudaMalloc'd buffers;
+// every GPU that loads the library holds it until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchDoubles = size_t(4) << 20;  // 4 Mi doubles = 32 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device addresses of g_noalloc_scratch, one per device (host code may not use
+// the symbol itself as a device pointer).
+constexpr int kNoAllocMaxDevices = 64;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+__global__ void k_noalloc_start_vector(double* x, size_t n) {
+  // Deterministic start vector with all modes excited (splitmix64 of the index).
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    unsigned long long z = (unsigned long long)i + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    x[i] = double(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  }
+}
+
+}  // namespace
+
+extern "C" int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* lmax) {
+  if (!h || !lmax || iters < 1) return TSP_ERR_ARG;
+  int rc;
+  if ((rc = begin(h))) return rc;
+  if (h->device < 0 || h->device >= kNoAllocMaxDevices)
+    return fail(h, TSP_ERR_UNSUPPORTED, "tsp_estimate_lmax_noalloc supports device ordinals 0..63");
+  const size_t n1 = size_t(h->ne) * h->R;  // one vector, layout [e][R]
+  if (2 * n1 + 3 > kNoAllocScratchDoubles)
+    return fail(h, TSP_ERR_ARG,
+                "tsp_estimate_lmax_noalloc: 2*ne*2Np + 3 = " + std::to_string(2 * n1 + 3) +
+                    " doubles exceed the fixed scratch of " + std::to_string(kNoAllocScratchDoubles) +
+                    " doubles (32 MiB); use tsp_estimate_lmax");
+  // One-time set-up per device, with that device current (begin() set it).
+  if (!g_noalloc_ptr[h->device]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(h, TSP_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[h->device] = static_cast<double*>(ptr);
+  }
+  double* da = g_noalloc_ptr[h->device];
+  double* db = da + n1;
+  double* dacc = db + n1;
+  k_noalloc_start_vector<<<592, 256, 0, h->stream>>>(da, n1);
+  TSP_CUDA(h, cudaGetLastError());
+  tsp::StepParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.ne = h->ne;
+  p.S = 1;
+  p.mode = tsp::kModePower;
+  p.row_ptr = h->d_row_ptr;
+  p.col = h->d_col;
+  p.blocks = h->d_blocks;
+  p.bpitch = h->bpitch;
+  p.bscale = (h->prec == TSP_PREC_BF16) ? h->d_bscale : nullptr;
+  p.minv = h->d_minv;
+  p.acc = dacc;
+  double scale = 1.0, lam = 0.0;
+  double acc[3];
+  for (int it = 0; it < iters; ++it) {
+    // The accumulators keep the previous call's values: clear them.
+    TSP_CUDA(h, cudaMemsetAsync(dacc, 0, 3 * sizeof(double), h->stream));
+    p.x = da;
+    p.out = db;
+    p.xscale = scale;
+    if ((rc = launch_step_params(h, p, h->stream))) return rc;
+    TSP_CUDA(h, cudaGetLastError());
+    TSP_CUDA(h, cudaMemcpyAsync(acc, dacc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
+    TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+    lam = acc[0] / acc[1];
+    scale = acc[2] > 0 ? 1.0 / std::sqrt(acc[2]) : 1.0;
+    std::swap(da, db);
+  }
+  *lmax = lam;
+  return TSP_OK;
+}
