@@ -238,3 +238,58 @@ def test_fp32_batched_pipeline_multi_tile(N):
     # the receivers after 120 steps), and the full fields of two shots.
     assert rel(lo, hi) < 1e-4
     assert rel(out["fp32"][1], out["fp64"][1]) < 1e-4 and rel(out["fp32"][2], out["fp64"][2]) < 1e-4
+
+
+def test_golden_run_matrix_free(golden):
+    """The matrix-free operator (no stored blocks) against the reference run."""
+    g = golden
+    s = capi.Simulation.create(g["xy"], g["tri"], int(g["N"]), g["lam"], g["mu"], g["rho"], [tuple(g["src"])],
+                               g["rcv"], penalty=float(g["penalty"]), op="matrix_free")
+    with s:
+        s.set_dt(float(g["dt"]))
+        f0, t0, amp, sdir = g["ricker"]
+        s.set_ricker(0, f0, t0, amp, int(sdir), int(g["nsteps"]))
+        s.first_step()
+        s.run(int(g["nsteps"]) - 1)
+        u = s.u()
+        seis = s.seismograms(0, int(g["nsteps"]))[0]
+    assert rel(u, g["u_final"]) < 1e-12
+    assert finite_rel(seis, g["seis"]) < 1e-12
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_matrix_free_apply_matches_explicit(N):
+    m = W.jittered_rect(5, 4, 500.0, 400.0, seed=N + 11)
+    rng = np.random.default_rng(N + 3)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    x = rng.standard_normal(2 * m.ne * (N + 1) * (N + 2) // 2)
+    ys = {}
+    for op in ("explicit", "matrix_free"):
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, [(250.0, 200.0)], [], penalty=10.0, op=op) as s:
+            ys[op] = (s.apply(x), s.estimate_lmax(300))
+    assert rel(ys["matrix_free"][0], ys["explicit"][0]) < 1e-13
+    assert abs(ys["matrix_free"][1] - ys["explicit"][1]) / ys["explicit"][1] < 1e-12
+
+
+def test_matrix_free_energy_and_resume():
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=8)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    rng = np.random.default_rng(2)
+    mk = lambda: capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, [(300.0, 200.0)],  # noqa: E731
+                                        W.surface_receivers(m, 3), penalty=10.0, op="matrix_free")
+    with mk() as a, mk() as b:
+        dt = 0.5 * 2 / np.sqrt(a.estimate_lmax(200))
+        u0 = 1e-3 * rng.standard_normal(2 * m.ne * 15)
+        for s in (a, b):
+            s.set_dt(dt)
+        a.set_initial(0, u0, None)
+        a.enable_energy(True)
+        a.first_step()
+        a.run(99)
+        E = a.energy(0, 100)
+        assert np.max(np.abs(E - E[0])) / E[0] < 1e-10
+        b.set_state(*a.get_state())
+        a.run(50)
+        b.run(50)
+        assert np.array_equal(a.u(), b.u())

@@ -35,6 +35,8 @@ struct tsp_handle {
   void* d_blocks = nullptr;
   float* d_bscale = nullptr;
   double* d_minv = nullptr;
+  // matrix-free operator: packed reference tables and per-element data
+  tsp::MatFreeParams mf = {};
   // state
   double* d_U[2] = {nullptr, nullptr};
   int cur = 0;  // d_U[cur] holds u^k, d_U[1-cur] holds u^{k-1}
@@ -200,6 +202,40 @@ int launch_batched(tsp_handle* h, const tsp::StepParams& p, dim3 grid, cudaStrea
   return TSP_OK;
 }
 
+template <int N>
+int launch_matfree_N(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::MFCfg<N> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_matfree<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("matrix-free kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tsp::k_step_matfree<N>, CF::WARPS * 32, smem);
+  if (per_sm < 1) per_sm = 1;
+  const long long want = (h->ne + CF::WARPS - 1) / CF::WARPS;
+  const unsigned grid = unsigned(std::min<long long>(want, (long long)per_sm * h->num_sms));
+  tsp::k_step_matfree<N><<<grid, CF::WARPS * 32, smem, st>>>(p, h->mf);
+  return TSP_OK;
+}
+
+int launch_matfree(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  switch (h->N) {
+    case 1: return launch_matfree_N<1>(h, p, st);
+    case 2: return launch_matfree_N<2>(h, p, st);
+    case 3: return launch_matfree_N<3>(h, p, st);
+    case 4: return launch_matfree_N<4>(h, p, st);
+    case 5: return launch_matfree_N<5>(h, p, st);
+    case 6: return launch_matfree_N<6>(h, p, st);
+    case 7: return launch_matfree_N<7>(h, p, st);
+    case 8: return launch_matfree_N<8>(h, p, st);
+    default: return fail(h, TSP_ERR_UNSUPPORTED, "matrix-free kernel: N must be in 1..8");
+  }
+}
+
 template <int R, int ST, int TR>
 int launch_pipe(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::PipeCfg<R, ST, TR> CF;
@@ -334,6 +370,7 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
     p.x32_out = h->d_X32[1 - ix];
   }
   if (mode == tsp::kModeApply || mode == tsp::kModePower) p.S = 1;  // single-vector products
+  if (h->op_kind == TSP_OP_MATRIX_FREE) return launch_matfree(h, p, st);
   switch (h->R) {
     case 6: return launch_R<6>(h, p, st);
     case 12: return launch_R<12>(h, p, st);
@@ -363,6 +400,7 @@ int block_pitch(int R, int S) { return S > 1 ? ((R + 3) & ~3) : R; }
 
 // Launches the step kernel family with fully prepared parameters.
 int launch_step_params(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  if (h->op_kind == TSP_OP_MATRIX_FREE) return launch_matfree(h, p, st);
   switch (h->R) {
     case 6: return launch_R<6>(h, p, st);
     case 12: return launch_R<12>(h, p, st);
@@ -472,8 +510,10 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   if (P->nshots < 1 || !P->src_xy) return fail(nullptr, TSP_ERR_ARG, "need nshots >= 1 and src_xy");
   if (P->nrcv < 0 || (P->nrcv > 0 && !P->rcv_xy)) return fail(nullptr, TSP_ERR_ARG, "bad receivers");
   if (P->precision < TSP_PREC_FP64 || P->precision > TSP_PREC_BF16) return fail(nullptr, TSP_ERR_ARG, "bad precision");
-  if (P->op_kind != TSP_OP_EXPLICIT)
-    return fail(nullptr, TSP_ERR_UNSUPPORTED, "matrix-free operator not available in this build");
+  if (P->op_kind != TSP_OP_EXPLICIT && P->op_kind != TSP_OP_MATRIX_FREE)
+    return fail(nullptr, TSP_ERR_ARG, "bad operator kind");
+  if (P->op_kind == TSP_OP_MATRIX_FREE && (P->precision != TSP_PREC_FP64 || P->nshots != 1))
+    return fail(nullptr, TSP_ERR_UNSUPPORTED, "the matrix-free operator runs FP64 with one shot per handle");
   for (int32_t i = 0; i < 3 * P->ne; ++i)
     if (P->tri[i] < 0 || P->tri[i] >= P->nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
   for (int32_t e = 0; e < P->ne; ++e)
@@ -559,6 +599,46 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
       (rc = upload(h, &d_Ds, T.Ds.data(), T.Ds.size())) || (rc = upload(h, &d_Dx, T.Dx.data(), T.Dx.size())))
     return create_error_from(h, rc);
   h->bpitch = block_pitch(h->R, h->S);
+  if (h->op_kind == TSP_OP_MATRIX_FREE) {
+    // Packed tables in the kernel's shared-memory layout: KT[ab][j][i],
+    // TRT[l][j][r], TR[l][r][i] (r < Q: basis, Q <= r < 3Q: gradient a = r/Q-1), w1.
+    const int Np = h->Np, Q = T.Q, Q3 = 3 * Q;
+    const size_t P2 = size_t(Np) * Np;
+    std::vector<double> pk(4 * P2 + 2 * size_t(3) * Np * Q3 + Q);
+    double* KT = pk.data();
+    double* TRT = KT + 4 * P2;
+    double* TR = TRT + size_t(3) * Np * Q3;
+    double* W1 = TR + size_t(3) * Q3 * Np;
+    for (int ab = 0; ab < 4; ++ab)
+      for (int i = 0; i < Np; ++i)
+        for (int j = 0; j < Np; ++j) KT[(size_t(ab) * Np + j) * Np + i] = T.K[ab * P2 + size_t(i) * Np + j];
+    for (int l = 0; l < 3; ++l)
+      for (int r = 0; r < Q3; ++r)
+        for (int j = 0; j < Np; ++j) {
+          const int kq = r % Q, part = r / Q;
+          const double v = part == 0 ? T.Be[(size_t(l) * Q + kq) * Np + j]
+                                     : T.Ge[((size_t(l) * 2 + (part - 1)) * Q + kq) * Np + j];
+          TRT[(size_t(l) * Np + j) * Q3 + r] = v;
+          TR[(size_t(l) * Q3 + r) * Np + j] = v;
+        }
+    for (int kq = 0; kq < Q; ++kq) W1[kq] = T.w1[kq];
+    double* d_tab = nullptr;
+    if ((rc = upload(h, &d_tab, pk.data(), pk.size()))) return create_error_from(h, rc);
+    h->mf.tables = d_tab;
+    h->mf.invJ = d_invJ;
+    h->mf.detJ = d_detJ;
+    h->mf.lam = d_lam;
+    h->mf.mu = d_mu;
+    h->mf.elen = d_elen;
+    h->mf.enrm = d_enrm;
+    h->mf.neigh = d_neigh;
+    h->mf.nedge = d_nedge;
+    h->mf.pen_n2 = P->penalty * h->N * h->N;
+    for (void* q : {(void*)d_bface, (void*)d_K, (void*)d_Ws, (void*)d_Wx, (void*)d_Ds, (void*)d_Dx}) dfree(h, q);
+    if ((rc = finish_create(h))) return create_error_from(h, rc);
+    *out = h;
+    return TSP_OK;
+  }
   const size_t RRp = size_t(h->R) * h->bpitch;
   const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
   {
@@ -1093,6 +1173,8 @@ int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax) {
 
 int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* blocks, double* minv) {
   if (!h) return TSP_ERR_ARG;
+  if (h->op_kind == TSP_OP_MATRIX_FREE && blocks)
+    return fail(h, TSP_ERR_UNSUPPORTED, "a matrix-free handle stores no blocks");
   int rc;
   if ((rc = begin(h))) return rc;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));

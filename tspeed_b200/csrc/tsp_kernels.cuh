@@ -105,6 +105,9 @@ struct AccOf { typedef float type; };
 template <>
 struct AccOf<double> { typedef double type; };
 
+// Parameters::avg_p (Parameters.cpp:37-45): harmonic mean, 0 when both are 0.
+__device__ __forceinline__ double harm(double a, double b) { return (a + b == 0) ? 0.0 : 2 * a * b / (a + b); }
+
 __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -1142,6 +1145,301 @@ __global__ void k_make_shadow(const double* __restrict__ u, float* __restrict__ 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Matrix-free step (FP64): the action of B on u^k is computed from the
+// factorised reference-element tables and per-element geometry/materials
+// instead of stored blocks. Same terms as the assembled operator
+// (Matrices_imp.hpp:22-215 with I <- I + I^T and B = pen N^2 S + I + A),
+// evaluated at quadrature points:
+//   volume   y^m += |detJ| sum_ab K^{ab} (sum_n alpha^{mn}_ab x^n)
+//   face l   with J^n(k) = u_e^n(k) - u_nb^n(Q-1-k) (jump at edge point k),
+//            T_e^m(k) = sum_{n,a} beta^{nm}_a(e) g_e^n_a(k) (traction of u_e),
+//            T_nb^m   = same on the neighbour's side with its own beta:
+//     y^m_i += sum_k w_k b_i(k) [pen N^2 sum_n c_mn J^n - L/2 (T_e^m - T_nb^m)]
+//            + sum_k w_k sum_a g^a_i(k) [-L/2 sum_n beta^{mn}_a(e) J^n]
+// One warp per element; persistent CTAs keep the tables in shared memory.
+// ---------------------------------------------------------------------------
+struct MatFreeParams {
+  const double* tables;  // packed KT | TRT | TR | w1 (see matfree_table_doubles)
+  const double* invJ;    // [ne][4]
+  const double* detJ;    // [ne]
+  const double* lam;     // [ne]
+  const double* mu;      // [ne]
+  const double* elen;    // [ne][3]
+  const double* enrm;    // [ne][3][2]
+  const int* neigh;      // [ne][3]
+  const int* nedge;      // [ne][3]
+  double pen_n2;
+};
+
+template <int N>
+struct MFCfg {
+  static constexpr int NP = (N + 1) * (N + 2) / 2;
+  static constexpr int Q = N + 1;
+  static constexpr int R = 2 * NP;
+  static constexpr int WARPS = 8;
+  static constexpr int KT = 4 * NP * NP;       // KT[ab][j][i]
+  static constexpr int TRT = 3 * NP * 3 * Q;   // TRT[l][j][r]
+  static constexpr int TR = 3 * 3 * Q * NP;    // TR[l][r][i]
+  static constexpr int TABLES = KT + TRT + TR + Q;
+  static constexpr int WS = 2 * NP + 2 * NP + 8 * NP + 2 * 3 * Q + 2 * 3 * Q + 6 * Q;  // per-warp scratch
+  static constexpr size_t smem_bytes() { return size_t(TABLES + WARPS * WS) * sizeof(double) + WARPS * sizeof(double); }
+};
+
+__device__ __forceinline__ void mf_beta(const MatFreeParams& q, int e, int l, double* beta /*[m][n][a]*/) {
+  const double lam = q.lam[e], mu = q.mu[e];
+  const double n0 = q.enrm[6 * size_t(e) + 2 * l], n1 = q.enrm[6 * size_t(e) + 2 * l + 1];
+  const double* iJ = q.invJ + 4 * size_t(e);
+  const double tau[4][2] = {{(lam + 2 * mu) * n0, mu * n1}, {lam * n1, mu * n0}, {mu * n1, lam * n0},
+                            {mu * n0, (lam + 2 * mu) * n1}};
+#pragma unroll
+  for (int mn = 0; mn < 4; ++mn)
+#pragma unroll
+    for (int a = 0; a < 2; ++a) beta[mn * 2 + a] = tau[mn][0] * iJ[a] + tau[mn][1] * iJ[a + 2];
+}
+
+template <int N>
+__global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const StepParams p, const MatFreeParams q) {
+  typedef MFCfg<N> CF;
+  constexpr int NP = CF::NP, Q = CF::Q, R = CF::R, Q3 = 3 * Q;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* tab = reinterpret_cast<double*>(smem_raw);
+  const double* KT = tab;
+  const double* TRT = KT + CF::KT;
+  const double* TR = TRT + CF::TRT;
+  const double* W1 = TR + CF::TR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* ws = tab + CF::TABLES + warp * CF::WS;
+  double* xe = ws;              // [2][NP]
+  double* xn = xe + 2 * NP;     // [2][NP]
+  double* zz = xn + 2 * NP;     // [8][NP]  z^{ab,m}, index (m*4 + ab)
+  double* TE = zz + 8 * NP;     // [2][3Q]
+  double* TN = TE + 2 * Q3;     // [2][3Q]
+  double* FH = TN + 2 * Q3;     // [6][Q]: F^0, F^1, H^0_0, H^0_1, H^1_0, H^1_1
+  double* red = tab + CF::TABLES + CF::WARPS * CF::WS;
+
+  for (int i = threadIdx.x; i < CF::TABLES; i += blockDim.x) tab[i] = q.tables[i];
+  __syncthreads();
+
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double dt = p.dt;
+  double en = 0.0, pw1 = 0.0, pw2 = 0.0;  // energy / power-iteration partials
+  const int gw = blockIdx.x * CF::WARPS + warp, nw = gridDim.x * CF::WARPS;
+  for (int e = gw; e < p.ne; e += nw) {
+    const double* xg = p.x + size_t(e) * R;
+    for (int t = lane; t < R; t += 32) {
+      double v = __ldg(xg + t);
+      if (p.mode == kModePower) v *= p.xscale;
+      xe[t] = v;
+    }
+    // alpha^{mn}_{ab} and z^{ab,m}_j = sum_n alpha^{mn}_ab x^n_j
+    {
+      const double lam = q.lam[e], mu = q.mu[e];
+      const double* iJ = q.invJ + 4 * size_t(e);
+      const double C[4][4] = {{lam + 2 * mu, 0, 0, mu}, {0, lam, mu, 0}, {0, mu, lam, 0}, {mu, 0, 0, lam + 2 * mu}};
+      double al[16];
+#pragma unroll
+      for (int mn = 0; mn < 4; ++mn)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            double s = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+              for (int ll = 0; ll < 2; ++ll) s += C[mn][kk * 2 + ll] * iJ[a + 2 * kk] * iJ[b + 2 * ll];
+            al[mn * 4 + a * 2 + b] = s;
+          }
+      __syncwarp();
+      for (int j = lane; j < NP; j += 32) {
+        const double x0 = xe[j], x1 = xe[NP + j];
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+          for (int ab = 0; ab < 4; ++ab) zz[(m * 4 + ab) * NP + j] = al[(m * 2 + 0) * 4 + ab] * x0 + al[(m * 2 + 1) * 4 + ab] * x1;
+      }
+    }
+    __syncwarp();
+    constexpr int RS = (NP + 31) / 32;  // row slots per lane
+    double acc[RS][2];
+#pragma unroll
+    for (int s = 0; s < RS; ++s) acc[s][0] = acc[s][1] = 0.0;
+    // ---- volume ----
+#pragma unroll
+    for (int s = 0; s < RS; ++s) {
+      const int i = lane + 32 * s;
+      if (i < NP) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int j = 0; j < NP; ++j) {
+#pragma unroll
+          for (int ab = 0; ab < 4; ++ab) {
+            const double kv = KT[(ab * NP + j) * NP + i];
+            a0 = fma(kv, zz[(0 * 4 + ab) * NP + j], a0);
+            a1 = fma(kv, zz[(1 * 4 + ab) * NP + j], a1);
+          }
+        }
+        const double adet = fabs(q.detJ[e]);
+        acc[s][0] = adet * a0;
+        acc[s][1] = adet * a1;
+      }
+    }
+    // ---- faces ----
+#pragma unroll 1
+    for (int l = 0; l < 3; ++l) {
+      const int nb = q.neigh[3 * size_t(e) + l];
+      if (nb < 0) continue;
+      const int lp = q.nedge[3 * size_t(e) + l];
+      const double* xgn = p.x + size_t(nb) * R;
+      for (int t = lane; t < R; t += 32) {
+        double v = __ldg(xgn + t);
+        if (p.mode == kModePower) v *= p.xscale;
+        xn[t] = v;
+      }
+      __syncwarp();
+      // Traces: values and reference gradients at the edge points, both sides.
+      for (int task = lane; task < 2 * Q3; task += 32) {
+        const bool self = task < Q3;
+        const int r = self ? task : task - Q3;
+        const double* T = TRT + (self ? l : lp) * NP * Q3;
+        const double* xv = self ? xe : xn;
+        double v0 = 0.0, v1 = 0.0;
+        for (int j = 0; j < NP; ++j) {
+          const double tv = T[j * Q3 + r];
+          v0 = fma(tv, xv[j], v0);
+          v1 = fma(tv, xv[NP + j], v1);
+        }
+        double* out = self ? TE : TN;
+        out[r] = v0;
+        out[Q3 + r] = v1;
+      }
+      __syncwarp();
+      if (lane < Q) {
+        const int kq = lane, kk = Q - 1 - lane;
+        double be[8], bn[8];
+        mf_beta(q, e, l, be);
+        mf_beta(q, nb, lp, bn);
+        const double al_ = harm(q.lam[e], q.lam[nb]), am_ = harm(q.mu[e], q.mu[nb]);
+        const double n0 = q.enrm[6 * size_t(e) + 2 * l], n1 = q.enrm[6 * size_t(e) + 2 * l + 1];
+        const double c00 = (al_ + 2 * am_) * n0 * n0 + 2 * am_ * n1 * n1;
+        const double c11 = (al_ + 2 * am_) * n1 * n1 + 2 * am_ * n0 * n0;
+        const double c01 = al_ * n0 * n1;
+        const double L = q.elen[3 * size_t(e) + l];
+        const double w = W1[kq];
+        const double J0 = TE[kq] - TN[kk], J1 = TE[Q3 + kq] - TN[Q3 + kk];
+        double Te[2], Tn[2];
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          double se = 0.0, sn = 0.0;
+#pragma unroll
+          for (int n = 0; n < 2; ++n)
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+              se += be[(n * 2 + m) * 2 + a] * TE[n * Q3 + (1 + a) * Q + kq];
+              sn += bn[(n * 2 + m) * 2 + a] * TN[n * Q3 + (1 + a) * Q + kk];
+            }
+          Te[m] = se;
+          Tn[m] = sn;
+        }
+        FH[0 * Q + kq] = w * (q.pen_n2 * (c00 * J0 + c01 * J1) - 0.5 * L * (Te[0] - Tn[0]));
+        FH[1 * Q + kq] = w * (q.pen_n2 * (c01 * J0 + c11 * J1) - 0.5 * L * (Te[1] - Tn[1]));
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+          for (int a = 0; a < 2; ++a)
+            FH[(2 + m * 2 + a) * Q + kq] =
+                -0.5 * L * w * (be[(m * 2 + 0) * 2 + a] * J0 + be[(m * 2 + 1) * 2 + a] * J1);
+      }
+      __syncwarp();
+      const double* T = TR + l * Q3 * NP;
+#pragma unroll
+      for (int s = 0; s < RS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < NP) {
+          double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+          for (int kq = 0; kq < Q; ++kq) {
+            const double bv = T[kq * NP + i], g0 = T[(Q + kq) * NP + i], g1 = T[(2 * Q + kq) * NP + i];
+            a0 += bv * FH[0 * Q + kq] + g0 * FH[2 * Q + kq] + g1 * FH[3 * Q + kq];
+            a1 += bv * FH[1 * Q + kq] + g0 * FH[4 * Q + kq] + g1 * FH[5 * Q + kq];
+          }
+          acc[s][0] += a0;
+          acc[s][1] += a1;
+        }
+      }
+      __syncwarp();
+    }
+    // ---- epilogue (rows i: component 0 at i, component 1 at NP + i) ----
+    const double mi = p.minv[e];
+    const bool is_src = (p.src_elem != nullptr) && (p.src_elem[0] == e) && (k < p.nF) &&
+                        (p.mode == kModeStep || p.mode == kModeFirst);
+    double* og = p.out + size_t(e) * R;
+#pragma unroll
+    for (int s = 0; s < RS; ++s) {
+      const int i = lane + 32 * s;
+      if (i >= NP) continue;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int r = c * NP + i;
+        const double y = acc[s][c];
+        const double u = xe[r];
+        double un;
+        if (p.mode == kModeStep || p.mode == kModeFirst) {
+          const double f = is_src ? p.F[2 * k + c] * p.src_phi[i] : 0.0;
+          if (p.mode == kModeStep) un = (2 * u - p.uprev[size_t(e) * R + r]) + mi * ((-dt * dt) * (y - f));
+          else un = (u + dt * (p.uprev ? p.uprev[size_t(e) * R + r] : 0.0)) - mi * (dt * dt / 2 * (y - f));
+          if (p.energy != nullptr) {
+            const double d = un - u;
+            en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un * y;
+          }
+        } else if (p.mode == kModeApply) {
+          un = y;
+        } else {  // kModePower
+          un = mi * y;
+          en += u * y;
+          pw1 += u * u / mi;
+          pw2 += un * un;
+        }
+        og[r] = un;
+      }
+    }
+    // receivers of this element
+    if (p.rcv_ptr != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
+      const int r0 = p.rcv_ptr[e], r1 = p.rcv_ptr[e + 1];
+      if (r1 > r0) {
+        __syncwarp();  // og written by the whole warp
+        const long long slot = k % p.seis_cap;
+        for (int t = lane; t < 2 * (r1 - r0); t += 32) {
+          const int rid = p.rcv_id[r0 + t / 2], c = t & 1;
+          const double* ph = p.rcv_phi + size_t(rid) * NP;
+          double v = 0.0;
+          for (int i = 0; i < NP; ++i) v += ph[i] * og[c * NP + i];
+          p.seis[(size_t(slot) * p.nrcv + rid) * 2 + c] = v;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (p.mode == kModePower) {
+    const double v0 = warp_sum(en), v1 = warp_sum(pw1), v2 = warp_sum(pw2);
+    if (lane == 0) {
+      atomicAdd(p.acc + 0, v0);
+      atomicAdd(p.acc + 1, v1);
+      atomicAdd(p.acc + 2, v2);
+    }
+  } else if (p.energy != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
+    const double v = warp_sum(en);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < CF::WARPS; ++w) sum += red[w];
+      atomicAdd(p.energy + (k % p.energy_cap), sum);
+    }
+  }
+}
+
 __global__ void k_advance(long long* step, long long n) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *step += n;
 }
@@ -1193,7 +1491,6 @@ struct AssembleParams {
   float* scale;              // [nnzb] (bf16)
 };
 
-__device__ __forceinline__ double harm(double a, double b) { return (a + b == 0) ? 0.0 : 2 * a * b / (a + b); }
 
 // beta^{mn}_a for element e, face l: out[(m*2+n)*2 + a]
 __device__ __forceinline__ void face_beta(const AssembleParams& p, int e, int l, double* beta) {
