@@ -203,6 +203,50 @@ def reference_arm(args):
     return 0
 
 
+def single_shot_forms(args):
+    """Single-shot configurations (2: 160k triangles N=6; 5: 655k triangles
+    N=6) with several operator forms on the same inputs: time per step,
+    DOF-steps/s, HBM roofline of the explicit forms, and the seismogram error
+    of every form against explicit FP64 over the timed steps."""
+    k = int(args.workload[-1])
+    prob = W.config(k, scale=args.scale)
+    K, Wm = args.steps, max(3, args.warmup)
+    hbm, peak_kind = peaks()
+    out = {"metric": "DOF-steps/s per operator form (single shot)", "unit": UNIT, "workload": args.workload,
+           "mesh_triangles": prob.mesh.ne, "N": prob.N, "dofs": prob.dofs_per_shot, "steps": K, "warmup": Wm,
+           "forms": {}}
+    dt = None
+    seis = {}
+    for form in args.forms.split(","):
+        op, prec = form.split("-")
+        with capi.Simulation.from_problem(prob, precision=prec, op=op) as s:
+            if dt is None:
+                dt, _ = estimate_dt(s)
+            prepare(s, prob, dt, K + Wm + 2)
+            s.set_seismogram_capacity(K + Wm + 2)
+            s.first_step()
+            s.run(Wm)
+            s.run_timed(K)
+            ms = s.run_timed(K)
+            seis[form] = s.seismograms(0, Wm + 2 * K + 1)
+            nnzb = s.nnzb
+        d = {"ms_per_step": ms / K, "value": prob.dofs_per_shot * K / (ms / 1e3)}
+        if op == "explicit":
+            algo = bytes_per_step(prob.mesh.ne, prob.Np, nnzb, 1, prec)
+            d["roofline_frac"] = algo / (ms / K / 1e3) / 1e9 / hbm
+            d["algorithmic_bytes_per_step"] = algo
+        out["forms"][form] = d
+    ref = seis.get("explicit-fp64")
+    if ref is not None and np.linalg.norm(ref) > 0:
+        for form, sg in seis.items():
+            out["forms"][form]["seismogram_rel_l2_vs_explicit_fp64"] = float(np.linalg.norm(sg - ref) / np.linalg.norm(ref))
+    out["dt"] = dt
+    out["peak_gbs"] = hbm
+    out["peak_source"] = peak_kind
+    print(json.dumps(out))
+    return 0
+
+
 def config_dict(args, prob):
     d = {"workload": "64-shot batched DG leap-frog: 200x100 jittered squares (40,000 triangles), Dubiner N=5, "
                      "log-normal vp, 128 receivers, FP32 blocks / FP64 state",
@@ -223,9 +267,14 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-FP64, accuracy, e2e and CPU legs")
+    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config5"],
+                    help="config3: the 64-shot headline; config2/config5: single-shot forms side by side")
+    ap.add_argument("--forms", default="explicit-fp64,explicit-fp32,matrix_free-fp64")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload != "config3":
+        return single_shot_forms(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
