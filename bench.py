@@ -222,13 +222,14 @@ def single_shot_forms(args):
         with capi.Simulation.from_problem(prob, precision=prec, op=op) as s:
             if dt is None:
                 dt, _ = estimate_dt(s)
-            prepare(s, prob, dt, K + Wm + 2)
-            s.set_seismogram_capacity(K + Wm + 2)
+            total = Wm + 2 * K + 1
+            prepare(s, prob, dt, total)
+            s.set_seismogram_capacity(total)
             s.first_step()
             s.run(Wm)
             s.run_timed(K)
             ms = s.run_timed(K)
-            seis[form] = s.seismograms(0, Wm + 2 * K + 1)
+            seis[form] = s.seismograms(0, total)
             nnzb = s.nnzb
         d = {"ms_per_step": ms / K, "value": prob.dofs_per_shot * K / (ms / 1e3)}
         if op == "explicit":
