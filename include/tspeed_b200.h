@@ -233,6 +233,34 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
 /* Source and receiver location: elements and basis values. */
 int tsp_export_points(tsp_handle* h, int32_t* src_elem, double* src_phi, int32_t* rcv_elem, double* rcv_phi);
 
+/* ---- Multi-mesh batch --------------------------------------------------
+ * Many independent simulations of uneven size and degree advanced together
+ * (no counterpart in the reference, which runs one LeapFrog per process).
+ * Each problem has one source (nshots = 1); all share precision, operator
+ * kind and device. Meshes of one degree form one group (a concatenated,
+ * block-diagonal-by-mesh system with per-mesh dt and source); every step of
+ * every group is replayed from one CUDA graph by tsp_batch_run. */
+typedef struct tsp_batch tsp_batch;
+int tsp_batch_create(const tsp_problem* meshes, int32_t nmesh, tsp_batch** out);
+int tsp_batch_destroy(tsp_batch* b);
+const char* tsp_batch_last_error(const tsp_batch* b);
+/* Number of degree groups and the total DOFs over all meshes. */
+int tsp_batch_info(const tsp_batch* b, int32_t* ngroups, int64_t* total_dofs);
+/* Largest eigenvalue of M^-1 B of every mesh (power iteration per mesh). */
+int tsp_batch_estimate_lmax(tsp_batch* b, int32_t iters, double* lmax);
+/* Per-mesh dt[nmesh] and Ricker sources (arrays of nmesh; see tsp_set_ricker). */
+int tsp_batch_set_dt(tsp_batch* b, const double* dt);
+int tsp_batch_set_ricker(tsp_batch* b, const double* dt, const double* f0, const double* t0, const double* amp,
+                         const int32_t* direction, int64_t n);
+int tsp_batch_set_seismogram_capacity(tsp_batch* b, int64_t nsteps);
+/* Zero initial state, then LeapFrog::first_step on every mesh. */
+int tsp_batch_first_step(tsp_batch* b);
+int tsp_batch_run(tsp_batch* b, int64_t nsteps);
+int tsp_batch_run_timed(tsp_batch* b, int64_t nsteps, double* ms);
+/* One mesh's displacement (reference layout) and seismograms [k][rcv][2]. */
+int tsp_batch_get_u(tsp_batch* b, int32_t mesh, double* out);
+int tsp_batch_get_seismograms(tsp_batch* b, int32_t mesh, int64_t k0, int64_t nk, double* out);
+
 /* Host-side projection of initial data (FESpace::transform,
  * FESpace_imp.hpp:136-179): the caller evaluates its field at the physical
  * volume quadrature points (collapsed Gauss<N+1> rule, (N+1)^2 points per

@@ -71,6 +71,19 @@ SIGNATURES = {
     "tsp_estimate_lmax_noalloc": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "tsp_export_operator": (C.c_int, [C.c_void_p, _ip, _ip, _dp, _dp]),
     "tsp_export_points": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _dp]),
+    "tsp_batch_create": (C.c_int, [C.POINTER(TspProblem), C.c_int32, C.POINTER(C.c_void_p)]),
+    "tsp_batch_destroy": (C.c_int, [C.c_void_p]),
+    "tsp_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "tsp_batch_info": (C.c_int, [C.c_void_p, _ip, _lp]),
+    "tsp_batch_estimate_lmax": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "tsp_batch_set_dt": (C.c_int, [C.c_void_p, _dp]),
+    "tsp_batch_set_ricker": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _ip, C.c_int64]),
+    "tsp_batch_set_seismogram_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
+    "tsp_batch_first_step": (C.c_int, [C.c_void_p]),
+    "tsp_batch_run": (C.c_int, [C.c_void_p, C.c_int64]),
+    "tsp_batch_run_timed": (C.c_int, [C.c_void_p, C.c_int64, _dp]),
+    "tsp_batch_get_u": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "tsp_batch_get_seismograms": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, _dp]),
     "tsp_quadrature_points": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp]),
     "tsp_project": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
@@ -326,3 +339,90 @@ class Simulation:
         _check(lib().tsp_export_points(self._h, _i(se), _d(sp), _i(re) if self.nrcv else None,
                                        _d(rp) if self.nrcv else None), self._h)
         return se, sp, re, rp
+
+
+def _bcheck(rc: int, b=None):
+    if rc != 0:
+        raise TspError(rc, lib().tsp_batch_last_error(b).decode())
+
+
+class Batch:
+    """Many independent meshes of uneven size and degree, one source each,
+    advanced together (tsp_batch_*). Problems are workloads.Problem objects
+    with one source."""
+
+    def __init__(self, problems, precision="fp64", op="explicit", device=0):
+        self._keep = []
+        arr = (TspProblem * len(problems))()
+        for i, pr in enumerate(problems):
+            xy, tri = _f64(pr.mesh.xy), _i32(pr.mesh.tri)
+            lam, mu, rho = _f64(pr.lam), _f64(pr.mu), _f64(pr.rho)
+            src = _f64(np.array([[pr.sources[0].x, pr.sources[0].y]]))
+            rcv = _f64(np.asarray(pr.receivers, dtype=np.float64).reshape(-1, 2))
+            self._keep += [xy, tri, lam, mu, rho, src, rcv]
+            arr[i] = TspProblem(xy.shape[0], _d(xy), tri.shape[0], _i(tri), pr.N, _d(lam), _d(mu), _d(rho),
+                                pr.penalty, TSP_PREC[precision], TSP_OP[op], 1, _d(src), rcv.shape[0],
+                                _d(rcv) if rcv.shape[0] else None, device)
+        h = C.c_void_p()
+        _bcheck(lib().tsp_batch_create(arr, len(problems), C.byref(h)))
+        self._b = h
+        self.problems = problems
+        self._keep = []
+        ng, td = C.c_int32(), C.c_int64()
+        _bcheck(lib().tsp_batch_info(self._b, C.byref(ng), C.byref(td)), self._b)
+        self.ngroups, self.total_dofs = ng.value, td.value
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().tsp_batch_destroy(self._b)
+            self._b = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def estimate_lmax(self, iters=100):
+        out = np.zeros(len(self.problems))
+        _bcheck(lib().tsp_batch_estimate_lmax(self._b, iters, _d(out)), self._b)
+        return out
+
+    def set_dt(self, dt):
+        self.dt = _f64(dt)
+        _bcheck(lib().tsp_batch_set_dt(self._b, _d(self.dt)), self._b)
+
+    def set_ricker(self, n):
+        ps = self.problems
+        f0 = _f64([p.sources[0].f0 for p in ps])
+        t0 = _f64([p.sources[0].t0 for p in ps])
+        amp = _f64([p.sources[0].amp for p in ps])
+        di = _i32([p.sources[0].direction for p in ps])
+        _bcheck(lib().tsp_batch_set_ricker(self._b, _d(self.dt), _d(f0), _d(t0), _d(amp), _i(di), n), self._b)
+
+    def set_seismogram_capacity(self, n):
+        _bcheck(lib().tsp_batch_set_seismogram_capacity(self._b, n), self._b)
+
+    def first_step(self):
+        _bcheck(lib().tsp_batch_first_step(self._b), self._b)
+
+    def run(self, n):
+        _bcheck(lib().tsp_batch_run(self._b, n), self._b)
+
+    def run_timed(self, n):
+        ms = C.c_double()
+        _bcheck(lib().tsp_batch_run_timed(self._b, n, C.byref(ms)), self._b)
+        return ms.value
+
+    def u(self, m):
+        p = self.problems[m]
+        out = np.zeros(2 * p.mesh.ne * p.Np)
+        _bcheck(lib().tsp_batch_get_u(self._b, m, _d(out)), self._b)
+        return out
+
+    def seismograms(self, m, k0, nk):
+        out = np.zeros((nk, len(self.problems[m].receivers), 2))
+        _bcheck(lib().tsp_batch_get_seismograms(self._b, m, k0, nk, _d(out)), self._b)
+        return out

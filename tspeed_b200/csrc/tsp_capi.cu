@@ -37,6 +37,12 @@ struct tsp_handle {
   double* d_minv = nullptr;
   // matrix-free operator: packed reference tables and per-element data
   tsp::MatFreeParams mf = {};
+  // multi-mesh group (set by tsp_batch_create; null for ordinary handles)
+  double* d_dt_elem = nullptr;
+  int* d_src_of = nullptr;
+  int* d_mesh_of = nullptr;
+  double* d_xscale_mesh = nullptr;
+  int nmesh = 0;
   // state
   double* d_U[2] = {nullptr, nullptr};
   int cur = 0;  // d_U[cur] holds u^k, d_U[1-cur] holds u^{k-1}
@@ -370,6 +376,10 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
     p.x32_out = h->d_X32[1 - ix];
   }
   if (mode == tsp::kModeApply || mode == tsp::kModePower) p.S = 1;  // single-vector products
+  p.dt_elem = h->d_dt_elem;
+  p.src_of = h->d_src_of;
+  p.mesh_of = (mode == tsp::kModePower) ? h->d_mesh_of : nullptr;
+  p.xscale_mesh = (mode == tsp::kModePower) ? h->d_xscale_mesh : nullptr;
   if (h->op_kind == TSP_OP_MATRIX_FREE) return launch_matfree(h, p, st);
   switch (h->R) {
     case 6: return launch_R<6>(h, p, st);
@@ -1350,3 +1360,422 @@ extern "C" int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* l
   *lmax = lam;
   return TSP_OK;
 }
+
+
+// ---------------------------------------------------------------------------
+// Multi-mesh batch: independent meshes of uneven size and degree advanced
+// together. Meshes of one degree are concatenated into one group handle (a
+// block-diagonal-by-mesh system with per-element dt, per-element source
+// index and per-element mesh id); every step of every group is captured in
+// one CUDA graph.
+// ---------------------------------------------------------------------------
+struct tsp_batch {
+  int nmesh = 0;
+  std::vector<tsp_handle*> groups;     // one per degree present
+  std::vector<int> mesh_group;         // mesh -> group
+  std::vector<int> mesh_first;         // mesh -> first element in its group
+  std::vector<int> mesh_ne, mesh_Np;   // per mesh
+  std::vector<int> mesh_rcv0, mesh_nrcv;  // mesh -> first receiver id in its group, count
+  std::vector<int> group_first_mesh;   // group -> mesh ids in order
+  std::vector<std::vector<int>> group_meshes;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  std::map<long long, cudaGraphExec_t> graphs;
+  std::string err = "no error";
+};
+
+namespace {
+int bfail(tsp_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+void batch_clear_graphs(tsp_batch* b) {
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+}
+}  // namespace
+
+extern "C" {
+
+int tsp_batch_destroy(tsp_batch* b) {
+  if (!b) return TSP_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_clear_graphs(b);
+  for (tsp_handle* h : b->groups) tsp_destroy(h);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return TSP_OK;
+}
+
+const char* tsp_batch_last_error(const tsp_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int tsp_batch_create(const tsp_problem* meshes, int32_t nmesh, tsp_batch** out) {
+  if (!meshes || !out || nmesh < 1) return bfail(nullptr, TSP_ERR_ARG, "need nmesh >= 1 problems");
+  *out = nullptr;
+  const int prec = meshes[0].precision, op = meshes[0].op_kind, dev = meshes[0].device;
+  for (int m = 0; m < nmesh; ++m) {
+    const tsp_problem& P = meshes[m];
+    if (P.nshots != 1 || !P.src_xy) return bfail(nullptr, TSP_ERR_ARG, "each mesh of a batch has exactly one source");
+    if (P.precision != prec || P.op_kind != op || P.device != dev)
+      return bfail(nullptr, TSP_ERR_ARG, "all meshes of a batch share precision, operator kind and device");
+    if (P.N < 1 || P.N > tsp::kMaxN || P.ne <= 0 || P.nverts <= 0 || !P.xy || !P.tri || !P.lambda || !P.mu || !P.rho)
+      return bfail(nullptr, TSP_ERR_ARG, "mesh " + std::to_string(m) + ": bad problem");
+    if (P.nrcv < 0 || (P.nrcv > 0 && !P.rcv_xy)) return bfail(nullptr, TSP_ERR_ARG, "bad receivers");
+  }
+  tsp_batch* b = new tsp_batch();
+  b->nmesh = nmesh;
+  b->device = dev;
+  b->mesh_group.assign(nmesh, -1);
+  b->mesh_first.assign(nmesh, 0);
+  b->mesh_ne.assign(nmesh, 0);
+  b->mesh_Np.assign(nmesh, 0);
+  b->mesh_rcv0.assign(nmesh, 0);
+  b->mesh_nrcv.assign(nmesh, 0);
+  if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return bfail(nullptr, TSP_ERR_CUDA, "batch stream creation failed");
+  }
+  for (int N = 1; N <= tsp::kMaxN; ++N) {
+    std::vector<int> ms;
+    for (int m = 0; m < nmesh; ++m)
+      if (meshes[m].N == N) ms.push_back(m);
+    if (ms.empty()) continue;
+    const int g = int(b->groups.size());
+    const int Np = tsp::np_of(N);
+    // Concatenate the group's meshes (vertex ids offset, no shared vertices).
+    std::vector<double> xy, lam, mu, rho, src_phi, rcv_phi;
+    std::vector<int32_t> tri, src_of, mesh_of, rcv_elem;
+    std::vector<double> rcv_xy_dummy;
+    int vbase = 0, ebase = 0, rbase = 0;
+    for (size_t q = 0; q < ms.size(); ++q) {
+      const tsp_problem& P = meshes[ms[q]];
+      xy.insert(xy.end(), P.xy, P.xy + 2 * size_t(P.nverts));
+      for (int i = 0; i < 3 * P.ne; ++i) tri.push_back(P.tri[i] + vbase);
+      lam.insert(lam.end(), P.lambda, P.lambda + P.ne);
+      mu.insert(mu.end(), P.mu, P.mu + P.ne);
+      rho.insert(rho.end(), P.rho, P.rho + P.ne);
+      // Point location within the mesh only (meshes may overlap in space).
+      tsp::Geometry gq = tsp::make_geometry(P.ne, P.xy, P.tri);
+      std::vector<double> ph(Np);
+      const int se = tsp::locate_point(N, P.ne, P.xy, P.tri, gq, P.src_xy[0], P.src_xy[1], ph.data());
+      if (se < 0) {
+        tsp_batch_destroy(b);
+        return bfail(nullptr, TSP_ERR_NOT_FOUND, "mesh " + std::to_string(ms[q]) + ": source point not found");
+      }
+      src_of.resize(size_t(ebase) + P.ne, -1);
+      src_of[size_t(ebase) + se] = int(q);
+      src_phi.insert(src_phi.end(), ph.begin(), ph.end());
+      for (int r = 0; r < P.nrcv; ++r) {
+        const int re = tsp::locate_point(N, P.ne, P.xy, P.tri, gq, P.rcv_xy[2 * r], P.rcv_xy[2 * r + 1], ph.data());
+        if (re < 0) {
+          tsp_batch_destroy(b);
+          return bfail(nullptr, TSP_ERR_NOT_FOUND, "mesh " + std::to_string(ms[q]) + ": receiver not found");
+        }
+        rcv_elem.push_back(ebase + re);
+        rcv_phi.insert(rcv_phi.end(), ph.begin(), ph.end());
+      }
+      for (int e = 0; e < P.ne; ++e) mesh_of.push_back(int(q));
+      b->mesh_group[ms[q]] = g;
+      b->mesh_first[ms[q]] = ebase;
+      b->mesh_ne[ms[q]] = P.ne;
+      b->mesh_Np[ms[q]] = Np;
+      b->mesh_rcv0[ms[q]] = rbase;
+      b->mesh_nrcv[ms[q]] = P.nrcv;
+      vbase += P.nverts;
+      ebase += P.ne;
+      rbase += P.nrcv;
+    }
+    // Group handle from the concatenated mesh. Its own source/receiver search
+    // is replaced below by the per-mesh results.
+    const tsp_problem& P0 = meshes[ms[0]];
+    std::vector<double> sxy;
+    {
+      // A point inside element 0 of the group (its centroid) as placeholder source.
+      const double* a = &xy[2 * size_t(tri[0])];
+      const double* c1 = &xy[2 * size_t(tri[1])];
+      const double* c2 = &xy[2 * size_t(tri[2])];
+      sxy = {(a[0] + c1[0] + c2[0]) / 3.0, (a[1] + c1[1] + c2[1]) / 3.0};
+    }
+    tsp_problem G = {};
+    G.nverts = vbase;
+    G.xy = xy.data();
+    G.ne = ebase;
+    G.tri = tri.data();
+    G.N = N;
+    G.lambda = lam.data();
+    G.mu = mu.data();
+    G.rho = rho.data();
+    G.penalty = P0.penalty;
+    G.precision = prec;
+    G.op_kind = op;
+    G.nshots = 1;
+    G.src_xy = sxy.data();
+    G.nrcv = 0;
+    G.rcv_xy = nullptr;
+    G.device = dev;
+    tsp_handle* h = nullptr;
+    int rc = tsp_create(&G, &h);
+    if (rc) {
+      const std::string msg = std::string("group N=") + std::to_string(N) + ": " + tsp_last_error(nullptr);
+      tsp_batch_destroy(b);
+      return bfail(nullptr, rc, msg);
+    }
+    b->groups.push_back(h);
+    b->group_meshes.push_back(ms);
+    // Per-mesh sources and receivers, mesh ids, per-mesh power scales.
+    h->nmesh = int(ms.size());
+    h->src_elem.assign(1, -1);
+    h->src_phi = src_phi;  // [nmesh][Np], row = source index
+    h->rcv_elem = rcv_elem;
+    h->rcv_phi = rcv_phi;
+    h->nrcv = rbase;
+    dfree(h, h->d_src_phi);
+    dfree(h, h->d_rcv_ptr);
+    dfree(h, h->d_rcv_id);
+    dfree(h, h->d_rcv_phi);
+    h->d_rcv_ptr = nullptr;
+    h->d_rcv_id = nullptr;
+    h->d_rcv_phi = nullptr;
+    std::vector<double> ones(ms.size(), 1.0);
+    if ((rc = upload(h, &h->d_src_phi, src_phi.data(), src_phi.size())) ||
+        (rc = upload(h, &h->d_src_of, src_of.data(), src_of.size())) ||
+        (rc = upload(h, &h->d_mesh_of, mesh_of.data(), mesh_of.size())) ||
+        (rc = upload(h, &h->d_xscale_mesh, ones.data(), ones.size())) || (rc = build_receiver_csr(h)) ||
+        (rc = alloc_seis(h, h->seis_cap)) || (rc = dalloc(h, &h->d_dt_elem, size_t(ebase)))) {
+      const std::string msg = h->err;
+      tsp_batch_destroy(b);
+      return bfail(nullptr, rc, msg);
+    }
+    dfree(h, h->d_acc);
+    if ((rc = dalloc(h, &h->d_acc, 3 * ms.size()))) {
+      const std::string msg = h->err;
+      tsp_batch_destroy(b);
+      return bfail(nullptr, rc, msg);
+    }
+    cudaStreamSynchronize(h->stream);
+  }
+  *out = b;
+  return TSP_OK;
+}
+
+int tsp_batch_info(const tsp_batch* b, int32_t* ngroups, int64_t* total_dofs) {
+  if (!b) return TSP_ERR_ARG;
+  if (ngroups) *ngroups = int32_t(b->groups.size());
+  if (total_dofs) {
+    int64_t t = 0;
+    for (int m = 0; m < b->nmesh; ++m) t += 2 * int64_t(b->mesh_ne[m]) * b->mesh_Np[m];
+    *total_dofs = t;
+  }
+  return TSP_OK;
+}
+
+int tsp_batch_estimate_lmax(tsp_batch* b, int32_t iters, double* lmax) {
+  if (!b || !lmax || iters < 1) return TSP_ERR_ARG;
+  cudaSetDevice(b->device);
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    tsp_handle* h = b->groups[g];
+    const int nm = h->nmesh;
+    const size_t n1 = size_t(h->ne) * h->R;
+    double *da = nullptr, *db = nullptr;
+    int rc;
+    if ((rc = dalloc(h, &da, n1)) || (rc = dalloc(h, &db, n1))) return bfail(b, rc, h->err);
+    std::vector<double> x0(n1);
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    for (size_t i = 0; i < n1; ++i) {
+      st ^= st << 13;
+      st ^= st >> 7;
+      st ^= st << 17;
+      x0[i] = double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+    }
+    if (cudaMemcpy(da, x0.data(), n1 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bfail(b, TSP_ERR_CUDA, "upload of the start vector failed");
+    std::vector<double> scale(nm, 1.0), acc(3 * size_t(nm)), lam(nm, 0.0);
+    for (int it = 0; it < iters; ++it) {
+      if (cudaMemcpyAsync(h->d_xscale_mesh, scale.data(), nm * sizeof(double), cudaMemcpyHostToDevice, h->stream) !=
+              cudaSuccess ||
+          cudaMemsetAsync(h->d_acc, 0, 3 * size_t(nm) * sizeof(double), h->stream) != cudaSuccess)
+        return bfail(b, TSP_ERR_CUDA, "power iteration setup failed");
+      if ((rc = launch_step(h, tsp::kModePower, da, nullptr, db, 0, 1.0, h->stream))) return bfail(b, rc, h->err);
+      if (cudaMemcpyAsync(acc.data(), h->d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return bfail(b, TSP_ERR_CUDA, std::string("power iteration: ") + cudaGetErrorString(cudaGetLastError()));
+      for (int q = 0; q < nm; ++q) {
+        lam[q] = acc[3 * q] / acc[3 * q + 1];
+        scale[q] = acc[3 * q + 2] > 0 ? 1.0 / std::sqrt(acc[3 * q + 2]) : 1.0;
+      }
+      std::swap(da, db);
+    }
+    for (int q = 0; q < nm; ++q) lmax[b->group_meshes[g][q]] = lam[q];
+    dfree(h, da);
+    dfree(h, db);
+  }
+  return TSP_OK;
+}
+
+int tsp_batch_set_dt(tsp_batch* b, const double* dt) {
+  if (!b || !dt) return TSP_ERR_ARG;
+  for (int m = 0; m < b->nmesh; ++m)
+    if (!(dt[m] > 0) || !std::isfinite(dt[m])) return bfail(b, TSP_ERR_ARG, "dt must be positive and finite");
+  cudaSetDevice(b->device);
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    tsp_handle* h = b->groups[g];
+    std::vector<double> de(h->ne);
+    for (int q = 0; q < h->nmesh; ++q) {
+      const int m = b->group_meshes[g][q];
+      for (int e = 0; e < b->mesh_ne[m]; ++e) de[b->mesh_first[m] + e] = dt[m];
+    }
+    if (cudaMemcpy(h->d_dt_elem, de.data(), de.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bfail(b, TSP_ERR_CUDA, "dt upload failed");
+    h->dt = dt[b->group_meshes[g][0]];  // the handle's own dt is unused by its kernels
+    h->dt_set = true;
+    clear_graphs(h);
+  }
+  batch_clear_graphs(b);
+  return TSP_OK;
+}
+
+int tsp_batch_set_ricker(tsp_batch* b, const double* dt, const double* f0, const double* t0, const double* amp,
+                         const int32_t* dir, int64_t n) {
+  if (!b || !dt || !f0 || !t0 || !amp || !dir || n < 1) return TSP_ERR_ARG;
+  cudaSetDevice(b->device);
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    tsp_handle* h = b->groups[g];
+    // Source rows are the group's meshes in order: a [nmesh][n][2] table.
+    std::vector<double> F(size_t(h->nmesh) * n * 2, 0.0), ts(n);
+    for (int q = 0; q < h->nmesh; ++q) {
+      const int m = b->group_meshes[g][q];
+      if (dir[m] != 0 && dir[m] != 1) return bfail(b, TSP_ERR_ARG, "direction must be 0 or 1");
+      tsp::force_times(dt[m], n, ts.data());
+      for (int64_t k = 0; k < n; ++k) F[(size_t(q) * n + k) * 2 + dir[m]] = tsp::ricker(ts[k], f0[m], t0[m], amp[m]);
+    }
+    dfree(h, h->d_F);
+    h->d_F = nullptr;
+    h->nF = n;
+    h->Fhost = F;
+    int rc;
+    if ((rc = upload(h, &h->d_F, F.data(), F.size()))) return bfail(b, rc, h->err);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bfail(b, TSP_ERR_CUDA, "force upload failed");
+    clear_graphs(h);
+  }
+  batch_clear_graphs(b);
+  return TSP_OK;
+}
+
+int tsp_batch_set_seismogram_capacity(tsp_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 1) return TSP_ERR_ARG;
+  for (tsp_handle* h : b->groups) {
+    int rc = tsp_set_seismogram_capacity(h, nsteps);
+    if (rc) return bfail(b, rc, h->err);
+  }
+  batch_clear_graphs(b);
+  return TSP_OK;
+}
+
+int tsp_batch_first_step(tsp_batch* b) {
+  if (!b) return TSP_ERR_ARG;
+  for (tsp_handle* h : b->groups) {
+    int rc;
+    if ((rc = tsp_set_initial(h, 0, nullptr, nullptr))) return bfail(b, rc, h->err);
+    if ((rc = tsp_first_step(h))) return bfail(b, rc, h->err);
+  }
+  for (tsp_handle* h : b->groups)
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bfail(b, TSP_ERR_CUDA, "first step failed");
+  return TSP_OK;
+}
+
+// All groups' steps in one graph, replayed on the batch stream.
+int tsp_batch_run(tsp_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 0) return TSP_ERR_ARG;
+  if (nsteps == 0) return TSP_OK;
+  cudaSetDevice(b->device);
+  for (tsp_handle* h : b->groups) {
+    if (h->steps_done < 1) return bfail(b, TSP_ERR_STATE, "run before first_step");
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bfail(b, TSP_ERR_CUDA, "group stream failed");
+  }
+  // Key: step count and the parity of every group's current level.
+  long long key = nsteps * 2 + b->groups[0]->cur;
+  auto it = b->graphs.find(key);
+  if (it == b->graphs.end()) {
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return bfail(b, TSP_ERR_CUDA, "batch graph capture failed to start");
+    int lrc = TSP_OK;
+    for (int64_t i = 0; i < nsteps && lrc == TSP_OK; ++i)
+      for (tsp_handle* h : b->groups) {
+        const int c = (h->cur + int(i & 1)) & 1;
+        lrc = launch_step(h, tsp::kModeStep, h->d_U[c], h->d_U[1 - c], h->d_U[1 - c], int(i), 1.0, b->stream);
+        if (lrc) break;
+      }
+    for (tsp_handle* h : b->groups) tsp::k_advance<<<1, 1, 0, b->stream>>>(h->d_step, nsteps);
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+    if (lrc) return bfail(b, lrc, "batch capture: kernel launch failed");
+    if (ce != cudaSuccess) return bfail(b, TSP_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+    cudaGraphExec_t exec;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return bfail(b, TSP_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(ce));
+    it = b->graphs.emplace(key, exec).first;
+  }
+  if (cudaGraphLaunch(it->second, b->stream) != cudaSuccess) return bfail(b, TSP_ERR_CUDA, "batch graph launch failed");
+  for (tsp_handle* h : b->groups) {
+    if (nsteps & 1) h->cur = 1 - h->cur;
+    h->steps_done += nsteps;
+  }
+  return TSP_OK;
+}
+
+int tsp_batch_run_timed(tsp_batch* b, int64_t nsteps, double* ms) {
+  if (!b || !ms) return TSP_ERR_ARG;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, b->stream);
+  int rc = tsp_batch_run(b, nsteps);
+  float f = 0.f;
+  if (rc == TSP_OK) {
+    cudaEventRecord(e1, b->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&f, e0, e1) != cudaSuccess)
+      rc = bfail(b, TSP_ERR_CUDA, "batch timing failed");
+  }
+  *ms = f;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+int tsp_batch_get_u(tsp_batch* b, int32_t mesh, double* out) {
+  if (!b || !out || mesh < 0 || mesh >= b->nmesh) return TSP_ERR_ARG;
+  tsp_handle* h = b->groups[b->mesh_group[mesh]];
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  const int Np = h->Np, R = h->R, ne = b->mesh_ne[mesh];
+  std::vector<double> v(size_t(ne) * R);
+  if (cudaMemcpy(v.data(), h->d_U[h->cur] + size_t(b->mesh_first[mesh]) * R, v.size() * sizeof(double),
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return bfail(b, TSP_ERR_CUDA, "state read-back failed");
+  for (int e = 0; e < ne; ++e)
+    for (int c = 0; c < 2; ++c)
+      std::memcpy(out + size_t(c) * ne * Np + size_t(e) * Np, &v[size_t(e) * R + size_t(c) * Np], Np * sizeof(double));
+  return TSP_OK;
+}
+
+int tsp_batch_get_seismograms(tsp_batch* b, int32_t mesh, int64_t k0, int64_t nk, double* out) {
+  if (!b || mesh < 0 || mesh >= b->nmesh || k0 < 0 || nk < 0 || (nk > 0 && !out)) return TSP_ERR_ARG;
+  tsp_handle* h = b->groups[b->mesh_group[mesh]];
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  const int nr = b->mesh_nrcv[mesh], r0 = b->mesh_rcv0[mesh];
+  if (nr == 0 || nk == 0) return TSP_OK;
+  if (nk > h->seis_cap) return bfail(b, TSP_ERR_ARG, "range longer than the seismogram capacity");
+  std::vector<double> all(size_t(nk) * h->nrcv * 2);
+  int rc = tsp_get_seismograms(h, k0, nk, all.data());
+  if (rc) return bfail(b, rc, h->err);
+  for (int64_t k = 0; k < nk; ++k)
+    std::memcpy(out + size_t(k) * nr * 2, &all[(size_t(k) * h->nrcv + r0) * 2], size_t(nr) * 2 * sizeof(double));
+  return TSP_OK;
+}
+
+}  // extern "C"

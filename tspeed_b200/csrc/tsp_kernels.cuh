@@ -66,6 +66,12 @@ struct StepParams {
   // neighbour gathers, x32_out receives u^{k+1}.
   const float* x32_in;
   float* x32_out;
+  // Multi-mesh groups (several independent meshes concatenated into one
+  // block-diagonal system; null for an ordinary handle):
+  const double* dt_elem;      // per-element time step (the element's mesh's dt)
+  const int* src_of;          // per-element source index into src_phi/F, -1 if none
+  const int* mesh_of;         // per-element mesh id (power iteration per mesh)
+  const double* xscale_mesh;  // per-mesh power-iteration scale
 };
 
 // ---------------------------------------------------------------------------
@@ -163,9 +169,10 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
     for (int b = 0; b < nb; ++b) {
       const int c = p.col[rb + b];
       const double2* src = reinterpret_cast<const double2*>(p.x + (size_t(c) * S + sh) * R);
+      const double xs = (p.mode == kModePower) ? (p.xscale_mesh ? p.xscale_mesh[p.mesh_of[e]] : p.xscale) : 1.0;
       for (int q = tl; q < NPAIR; q += T) {
         double2 v = __ldg(src + q);
-        if (p.mode == kModePower) { v.x *= p.xscale; v.y *= p.xscale; }
+        if (p.mode == kModePower) { v.x *= xs; v.y *= xs; }
         xt[b][2 * q] = v.x;
         xt[b][2 * q + 1] = v.y;
       }
@@ -224,14 +231,16 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   double en2 = 0.0, en3 = 0.0;
   if (active) {
     const double mi = p.minv[e];
-    const bool is_src = (p.src_elem != nullptr) && (p.src_elem[sh] == e) && (k < p.nF) &&
-                        (p.mode == kModeStep || p.mode == kModeFirst);
+    // Source row: the shot's own source (one per shot), or in a multi-mesh
+    // group the source of this element's mesh.
+    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && p.src_elem[sh] == e) ? sh : -1);
+    const bool is_src = (srow >= 0) && (k < p.nF) && (p.mode == kModeStep || p.mode == kModeFirst);
     double Fk[2] = {0.0, 0.0};
     if (is_src) {
-      Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
-      Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+      Fk[0] = p.F[(size_t(srow) * p.nF + k) * 2];
+      Fk[1] = p.F[(size_t(srow) * p.nF + k) * 2 + 1];
     }
-    const double dt = p.dt;
+    const double dt = p.dt_elem ? p.dt_elem[e] : p.dt;
 #pragma unroll
     for (int s = 0; s < PPL; ++s) {
       const int q = tl + T * s;
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
         for (int h = 0; h < 2; ++h) {
           const int r = 2 * q + h;
           const int comp = r / NP, i = r - comp * NP;
-          f[h] = Fk[comp] * p.src_phi[size_t(sh) * NP + i];
+          f[h] = Fk[comp] * p.src_phi[size_t(srow) * NP + i];
         }
       }
       if (p.mode == kModeStep) {
@@ -317,6 +326,29 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
     }
   }
 
+  // ---- per-mesh power-iteration sums (multi-mesh groups) ----
+  if (p.mode == kModePower && p.mesh_of != nullptr) {
+    // Team-segmented sum through shared memory: teams of one warp can
+    // belong to different meshes.
+    __shared__ double tsum[RT::WARPS][32][3];
+    tsum[warp][lane][0] = en;
+    tsum[warp][lane][1] = en2;
+    tsum[warp][lane][2] = en3;
+    __syncwarp();
+    if (active && tl == 0) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      for (int l2 = 0; l2 < T; ++l2) {
+        a0 += tsum[warp][tw * T + l2][0];
+        a1 += tsum[warp][tw * T + l2][1];
+        a2 += tsum[warp][tw * T + l2][2];
+      }
+      double* acc3 = p.acc + 3 * size_t(p.mesh_of[e]);
+      atomicAdd(acc3 + 0, a0);
+      atomicAdd(acc3 + 1, a1);
+      atomicAdd(acc3 + 2, a2);
+    }
+    return;
+  }
   // ---- block reductions (energy, power iteration) ----
   if (p.mode == kModePower || p.energy != nullptr) {
     const int nred = (p.mode == kModePower) ? 3 : 1;
@@ -1223,14 +1255,14 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
   __syncthreads();
 
   const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
-  const double dt = p.dt;
   double en = 0.0, pw1 = 0.0, pw2 = 0.0;  // energy / power-iteration partials
   const int gw = blockIdx.x * CF::WARPS + warp, nw = gridDim.x * CF::WARPS;
   for (int e = gw; e < p.ne; e += nw) {
     const double* xg = p.x + size_t(e) * R;
+    const double xsc = (p.mode == kModePower) ? (p.xscale_mesh ? p.xscale_mesh[p.mesh_of[e]] : p.xscale) : 1.0;
     for (int t = lane; t < R; t += 32) {
       double v = __ldg(xg + t);
-      if (p.mode == kModePower) v *= p.xscale;
+      if (p.mode == kModePower) v *= xsc;
       xe[t] = v;
     }
     // alpha^{mn}_{ab} and z^{ab,m}_j = sum_n alpha^{mn}_ab x^n_j
@@ -1294,7 +1326,7 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
       const double* xgn = p.x + size_t(nb) * R;
       for (int t = lane; t < R; t += 32) {
         double v = __ldg(xgn + t);
-        if (p.mode == kModePower) v *= p.xscale;
+        if (p.mode == kModePower) v *= xsc;  // neighbours belong to the same mesh
         xn[t] = v;
       }
       __syncwarp();
@@ -1372,9 +1404,11 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
     }
     // ---- epilogue (rows i: component 0 at i, component 1 at NP + i) ----
     const double mi = p.minv[e];
-    const bool is_src = (p.src_elem != nullptr) && (p.src_elem[0] == e) && (k < p.nF) &&
-                        (p.mode == kModeStep || p.mode == kModeFirst);
+    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && p.src_elem[0] == e) ? 0 : -1);
+    const bool is_src = (srow >= 0) && (k < p.nF) && (p.mode == kModeStep || p.mode == kModeFirst);
+    const double dt = p.dt_elem ? p.dt_elem[e] : p.dt;
     double* og = p.out + size_t(e) * R;
+    double ew = 0.0, pe0 = 0.0, pe1 = 0.0, pe2 = 0.0;  // this element's power-iteration sums
 #pragma unroll
     for (int s = 0; s < RS; ++s) {
       const int i = lane + 32 * s;
@@ -1386,7 +1420,7 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
         const double u = xe[r];
         double un;
         if (p.mode == kModeStep || p.mode == kModeFirst) {
-          const double f = is_src ? p.F[2 * k + c] * p.src_phi[i] : 0.0;
+          const double f = is_src ? p.F[(size_t(srow) * p.nF + k) * 2 + c] * p.src_phi[size_t(srow) * NP + i] : 0.0;
           if (p.mode == kModeStep) un = (2 * u - p.uprev[size_t(e) * R + r]) + mi * ((-dt * dt) * (y - f));
           else un = (u + dt * (p.uprev ? p.uprev[size_t(e) * R + r] : 0.0)) - mi * (dt * dt / 2 * (y - f));
           if (p.energy != nullptr) {
@@ -1397,11 +1431,27 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
           un = y;
         } else {  // kModePower
           un = mi * y;
-          en += u * y;
-          pw1 += u * u / mi;
-          pw2 += un * un;
+          pe0 += u * y;
+          pe1 += u * u / mi;
+          pe2 += un * un;
         }
         og[r] = un;
+      }
+    }
+    (void)ew;
+    if (p.mode == kModePower) {
+      if (p.mesh_of != nullptr) {
+        const double v0 = warp_sum(pe0), v1 = warp_sum(pe1), v2 = warp_sum(pe2);
+        if (lane == 0) {
+          double* acc3 = p.acc + 3 * size_t(p.mesh_of[e]);
+          atomicAdd(acc3 + 0, v0);
+          atomicAdd(acc3 + 1, v1);
+          atomicAdd(acc3 + 2, v2);
+        }
+      } else {
+        en += pe0;
+        pw1 += pe1;
+        pw2 += pe2;
       }
     }
     // receivers of this element
@@ -1421,7 +1471,7 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
     }
     __syncwarp();
   }
-  if (p.mode == kModePower) {
+  if (p.mode == kModePower && p.mesh_of == nullptr) {
     const double v0 = warp_sum(en), v1 = warp_sum(pw1), v2 = warp_sum(pw2);
     if (lane == 0) {
       atomicAdd(p.acc + 0, v0);
