@@ -203,6 +203,50 @@ def reference_arm(args):
     return 0
 
 
+def mesh_batch_forms(args):
+    """Config 4: 256 independent jittered meshes (500..20,000 triangles,
+    N in 3..8, own material, own Ricker source, per-mesh dt = 0.4 x CFL),
+    advanced together by one graph per step chunk. Forms: FP32 explicit
+    blocks vs the FP64 matrix-free operator (explicit FP64 blocks of this
+    batch, ~273 GB, do not fit in HBM). Seismogram error of the FP32 form
+    against FP64 over --accuracy-steps (default 400)."""
+    probs = W.mesh_batch(nmesh=256, scale=args.scale)
+    K, Wm = args.steps, max(3, args.warmup)
+    nacc = 400 if args.accuracy_steps < 0 else args.accuracy_steps
+    total = max(Wm + 2 * K + 1, nacc)
+    out = {"metric": "DOF-steps/s, uneven multi-mesh batch", "unit": UNIT, "workload": "config4",
+           "meshes": len(probs), "triangles": int(sum(p.mesh.ne for p in probs)),
+           "dofs": int(sum(p.dofs_per_shot for p in probs)), "steps": K, "warmup": Wm, "forms": {}}
+    dt = None
+    seis = {}
+    for form in ("matrix_free-fp64", "explicit-fp32"):
+        op, prec = form.split("-")
+        t0 = time.perf_counter()
+        with capi.Batch(probs, precision=prec, op=op) as b:
+            setup = time.perf_counter() - t0
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(b.estimate_lmax(60))
+            b.set_dt(dt)
+            b.set_ricker(total)
+            b.set_seismogram_capacity(total)
+            b.first_step()
+            b.run(Wm)
+            b.run_timed(K)
+            ms = b.run_timed(K)
+            done = 1 + Wm + 2 * K
+            if total > done:
+                b.run(total - done)
+            seis[form] = [b.seismograms(m, 0, total) for m in range(len(probs))]
+            dofs = b.total_dofs
+        out["forms"][form] = {"ms_per_step": ms / K, "value": dofs * K / (ms / 1e3), "setup_s": setup}
+    ref = np.concatenate([x.ravel() for x in seis["matrix_free-fp64"]])
+    lo = np.concatenate([x.ravel() for x in seis["explicit-fp32"]])
+    out["forms"]["explicit-fp32"]["seismogram_rel_l2_vs_fp64"] = float(np.linalg.norm(lo - ref) / np.linalg.norm(ref))
+    out["accuracy_steps"] = total
+    print(json.dumps(out))
+    return 0
+
+
 def single_shot_forms(args):
     """Single-shot configurations (2: 160k triangles N=6; 5: 655k triangles
     N=6) with several operator forms on the same inputs: time per step,
@@ -268,12 +312,14 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-FP64, accuracy, e2e and CPU legs")
-    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config5"],
+    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config4", "config5"],
                     help="config3: the 64-shot headline; config2/config5: single-shot forms side by side")
     ap.add_argument("--forms", default="explicit-fp64,explicit-fp32,matrix_free-fp64")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "config4":
+        return mesh_batch_forms(args)
     if args.workload != "config3":
         return single_shot_forms(args)
 
