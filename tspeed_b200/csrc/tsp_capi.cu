@@ -15,6 +15,7 @@
 #include "../../include/tspeed_b200.h"
 #include "tsp_host.h"
 #include "tsp_kernels.cuh"
+#include "tsp_tcgen05.cuh"
 
 namespace {
 
@@ -53,6 +54,7 @@ struct tsp_handle {
   // pipelined single group (2Np = 56); 1 pipelined single group; 2 the
   // non-persistent cp.async kernel. Selected by TSP_BATCHED_VARIANT.
   int kernel_variant = 0;
+  int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
   int num_sms = 148;
   long long* d_step = nullptr;
   // sources / receivers
@@ -177,6 +179,8 @@ int finish_create(tsp_handle* h) {
   }
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  if ((rc = dalloc(h, &h->d_err, 1))) return rc;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
   if ((rc = dalloc(h, &h->d_acc, 3))) return rc;
   if ((rc = upload(h, &h->d_src_elem, h->src_elem.data(), h->src_elem.size()))) return rc;
   if ((rc = upload(h, &h->d_src_phi, h->src_phi.data(), h->src_phi.size()))) return rc;
@@ -261,6 +265,29 @@ int launch_pipe(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 template <int R>
+int launch_tc(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::TcCfg<R> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e =
+        cudaFuncSetAttribute(tsp::k_step_batched_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("tensor-core kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  // Resident CTAs per SM, limited by shared memory and by tensor memory
+  // (512 columns per SM) so that no allocation ever waits.
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tsp::k_step_batched_tc<R>, CF::NT, smem);
+  per_sm = std::max(1, std::min(per_sm, 512 / CF::TCOLS));
+  const long long items = (long long)h->ne * ((h->S + CF::M - 1) / CF::M);
+  const unsigned grid = unsigned(std::min<long long>(items, (long long)per_sm * h->num_sms));
+  tsp::k_step_batched_tc<R><<<grid, CF::NT, smem, st>>>(p, h->d_err);
+  return TSP_OK;
+}
+
+template <int R>
 int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::KsplitCfg<R> CF;
   const size_t smem = CF::smem_bytes();
@@ -281,8 +308,11 @@ int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
+    if constexpr (R <= 56) {
+      if (h->kernel_variant == 3 && p.energy == nullptr) return launch_tc<R>(h, p, st);
+    }
     if constexpr (R <= 42) {
-      if (h->kernel_variant == 0) return launch_ksplit<R>(h, p, st);
+      if (h->kernel_variant == 0 || h->kernel_variant == 3) return launch_ksplit<R>(h, p, st);
       return launch_pipe<R, 64, 4>(h, p, st);
     } else if constexpr (R <= 56) {
       return launch_pipe<R, 32, 2>(h, p, st);
@@ -440,6 +470,15 @@ void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* ds
                   Np * sizeof(double));
 }
 
+
+// Reports a bounded device-side wait that gave up (after a synchronisation).
+int check_device_error(tsp_handle* h) {
+  if (!h->d_err) return TSP_OK;
+  int v = 0;
+  TSP_CUDA(h, cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) return fail(h, TSP_ERR_TIMEOUT, "a tensor-core step kernel timed out waiting for its MMAs; results invalid");
+  return TSP_OK;
+}
 
 // One shot's slice of a device state buffer (ne runs of R doubles with a
 // stride of S*R) to/from a reference-layout host vector (NULL: zeros).
@@ -976,6 +1015,7 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
     if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
     if (e != cudaSuccess) rc = fail(h, TSP_ERR_CUDA, std::string("timing events: ") + cudaGetErrorString(e));
     *ms = f;
+    if (rc == TSP_OK) rc = check_device_error(h);
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -994,7 +1034,8 @@ int tsp_get_u(tsp_handle* h, int32_t shot, double* out) {
   if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
   int rc;
   if ((rc = begin(h))) return rc;
-  return get_shot(h, h->d_U[h->cur], shot, out);
+  if ((rc = get_shot(h, h->d_U[h->cur], shot, out))) return rc;
+  return check_device_error(h);
 }
 
 int tsp_set_seismogram_capacity(tsp_handle* h, int64_t nsteps) {
