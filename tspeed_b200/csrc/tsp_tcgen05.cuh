@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(TcCfg<R>::NT) k_step_batched_tc(const StepPara
     *abort_s = 0;
     for (int i = 0; i < 2; ++i)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[i])), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_base_s)),
