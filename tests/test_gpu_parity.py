@@ -323,3 +323,73 @@ def test_tensor_core_batched_step(N, monkeypatch):
         assert rel(out["tc"][i], out["fp64"][i]) < 1e-4
         assert rel(out["tc"][i], out["simt"][i]) < 1e-4
     print("tc vs fp64:", rel(out["tc"][0], out["fp64"][0]), "simt vs fp64:", rel(out["simt"][0], out["fp64"][0]))
+
+
+@pytest.mark.parametrize("N", [2, 4, 5, 6])
+def test_fixed_point_tensor_core_step(N, monkeypatch):
+    """Tensor-core step with fixed-point BF16 slices and an exact main
+    product (variant 4), 70 shots (one full and one partial 64-shot tile):
+    within the 1e-4 budget of the FP64 batched path shot by shot, and as close
+    to it as the FP32 CUDA-core kernel is (within 10x of its error)."""
+    m = W.jittered_rect(8, 5, 800.0, 500.0, seed=N + 90)
+    rng = np.random.default_rng(N + 7)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    shots = [(40 + 720 * rng.random(), 40 + 420 * rng.random()) for _ in range(70)]
+    rcv = W.surface_receivers(m, 6)
+    n = 150
+    out = {}
+    dt = None
+    for tag, prec, variant in (("fp64", "fp64", "0"), ("simt", "fp32", "0"), ("fx", "fp32", "4")):
+        monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
+            s.set_dt(dt)
+            for k in range(70):
+                s.set_ricker(k, 25.0, 0.04, -1.0, k % 2, n)
+            s.first_step()
+            s.run(n - 1)
+            out[tag] = (s.seismograms(0, n), s.u(3), s.u(66))
+    errs = [(rel(out["fx"][i], out["fp64"][i]), rel(out["simt"][i], out["fp64"][i])) for i in range(3)]
+    print("N", N, "(fx, simt) vs fp64 for seismograms, u(3), u(66):", errs)
+    for e_fx, e_simt in errs:
+        assert e_fx < 1e-4 and e_fx < 10 * e_simt + 1e-9
+
+
+def test_fixed_point_tensor_core_resume_and_energy(monkeypatch):
+    """Variant 4: a checkpoint/resume in the middle continues bit-identically
+    (the state slices are rebuilt from the FP64 state with the epilogue's own
+    arithmetic), and without sources the discrete energy stays constant."""
+    monkeypatch.setenv("TSP_BATCHED_VARIANT", "4")
+    g = __import__("conftest").load_golden("g_config1_small")
+    shots = [tuple(g["src"]), (900.0, 700.0), (3100.0, 1200.0)]
+    n = int(g["nsteps"])
+    with sim_from_golden(g, "fp32", shots=shots) as a, sim_from_golden(g, "fp32", shots=shots) as b:
+        a.first_step()
+        a.run(40)
+        b.set_state(*a.get_state())
+        a.run(n - 41)
+        b.run(n - 41)
+        for k in range(3):
+            assert np.array_equal(a.u(k), b.u(k))
+        assert np.array_equal(a.seismograms(41, n - 41), b.seismograms(41, n - 41))
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=5)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    drift = {}
+    for variant in ("0", "4"):
+        monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+        with capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, [(300.0, 200.0), (150.0, 100.0), (450.0, 300.0)],
+                                    W.surface_receivers(m, 2), penalty=10.0, precision="fp32") as s:
+            rng = np.random.default_rng(3)
+            s.set_dt(0.4 * 2 / np.sqrt(s.estimate_lmax(100)))
+            for k in range(3):
+                s.set_initial(k, 1e-3 * rng.standard_normal(2 * s.ne * s.Np), None)
+            s.enable_energy(True)
+            s.first_step()
+            s.run(299)
+            E = s.energy(0, 300)
+        assert np.all(np.isfinite(E)) and E[0] > 0
+        drift[variant] = np.max(np.abs(E - E[0])) / E[0]
+    print("energy drift: simt", drift["0"], "fx", drift["4"])
+    assert drift["4"] < 1e-5

@@ -16,6 +16,7 @@
 #include "tsp_host.h"
 #include "tsp_kernels.cuh"
 #include "tsp_tcgen05.cuh"
+#include "tsp_tcfx.cuh"
 
 namespace {
 
@@ -54,6 +55,14 @@ struct tsp_handle {
   // pipelined single group (2Np = 56); 1 pipelined single group; 2 the
   // non-persistent cp.async kernel. Selected by TSP_BATCHED_VARIANT.
   int kernel_variant = 0;
+  // Tensor-core fixed-point step (variant 4): operator slice images and row
+  // scales, built once; state slice images and shot scales, one pair per
+  // state level like the FP32 shadow.
+  bool fx = false;
+  unsigned char* d_Bsl = nullptr;
+  int* d_Bex = nullptr;
+  unsigned char* d_Xsl[2] = {nullptr, nullptr};
+  int* d_Xex[2] = {nullptr, nullptr};
   int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
   int num_sms = 148;
   long long* d_step = nullptr;
@@ -158,6 +167,51 @@ int alloc_seis(tsp_handle* h, long long cap) {
   return TSP_OK;
 }
 
+template <int R>
+using FxDefault = tsp::FxCfg<R>;
+
+// State slices of level i from its FP64 values (padding stays zero).
+template <int R>
+int fx_refresh_R(tsp_handle* h, int i) {
+  tsp::k_make_xslices<R><<<1184, 128, 0, h->stream>>>(h->d_U[i], h->ne, h->S, h->d_Xsl[i], h->d_Xex[i]);
+  TSP_CUDA(h, cudaGetLastError());
+  return TSP_OK;
+}
+
+// Operator slice images from the stored FP32 blocks, state slice buffers.
+template <int R>
+int fx_setup_R(tsp_handle* h) {
+  typedef FxDefault<R> CF;
+  int rc;
+  const size_t bbytes = size_t(h->nnzb) * CF::BBYTES;
+  if ((rc = dalloc(h, &h->d_Bsl, bbytes)) || (rc = dalloc(h, &h->d_Bex, size_t(h->nnzb) * CF::GW))) return rc;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_Bsl, 0, bbytes, h->stream));
+  tsp::k_make_bslices<float, R><<<1184, 128, 0, h->stream>>>(
+      reinterpret_cast<const float*>(h->d_blocks), h->bpitch, h->nnzb, h->d_Bsl, h->d_Bex);
+  TSP_CUDA(h, cudaGetLastError());
+  const size_t ntile = size_t((h->S + 63) / 64);
+  const size_t xbytes = size_t(h->ne) * ntile * CF::ABYTES;
+  for (int i = 0; i < 2; ++i) {
+    if ((rc = dalloc(h, &h->d_Xsl[i], xbytes)) || (rc = dalloc(h, &h->d_Xex[i], size_t(h->ne) * ntile * 64)))
+      return rc;
+    TSP_CUDA(h, cudaMemsetAsync(h->d_Xsl[i], 0, xbytes, h->stream));
+    TSP_CUDA(h, cudaMemsetAsync(h->d_Xex[i], 0x80, size_t(h->ne) * ntile * 64 * sizeof(int), h->stream));
+  }
+  return TSP_OK;
+}
+
+int fx_dispatch(tsp_handle* h, bool setup, int i) {
+  switch (h->R) {
+    case 6: return setup ? fx_setup_R<6>(h) : fx_refresh_R<6>(h, i);
+    case 12: return setup ? fx_setup_R<12>(h) : fx_refresh_R<12>(h, i);
+    case 20: return setup ? fx_setup_R<20>(h) : fx_refresh_R<20>(h, i);
+    case 30: return setup ? fx_setup_R<30>(h) : fx_refresh_R<30>(h, i);
+    case 42: return setup ? fx_setup_R<42>(h) : fx_refresh_R<42>(h, i);
+    case 56: return setup ? fx_setup_R<56>(h) : fx_refresh_R<56>(h, i);
+    default: return fail(h, TSP_ERR_UNSUPPORTED, "no tensor-core step for 2Np = " + std::to_string(h->R));
+  }
+}
+
 // Common tail of both constructors: state, step counter, sources, receivers.
 int finish_create(tsp_handle* h) {
   int rc;
@@ -177,6 +231,8 @@ int finish_create(tsp_handle* h) {
       TSP_CUDA(h, cudaMemsetAsync(h->d_X32[i], 0, nsh * sizeof(float), h->stream));
     }
   }
+  h->fx = h->shadow && h->kernel_variant == 4 && h->op_kind == TSP_OP_EXPLICIT && h->R <= 56;
+  if (h->fx && (rc = fx_dispatch(h, true, 0))) return rc;
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
   if ((rc = dalloc(h, &h->d_err, 1))) return rc;
@@ -288,6 +344,26 @@ int launch_tc(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 template <int R>
+int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef FxDefault<R> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched_fx<R>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("tensor-core kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  // Persistent: one CTA per SM (its shared memory and, for 2Np >= 42, its
+  // 512 tensor-memory columns admit no second one).
+  const long long items = (long long)h->ne * ((h->S + CF::M - 1) / CF::M);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched_fx<R><<<grid, CF::NT, smem, st>>>(p, h->d_err);
+  return TSP_OK;
+}
+
+template <int R>
 int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::KsplitCfg<R> CF;
   const size_t smem = CF::smem_bytes();
@@ -307,6 +383,9 @@ int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 
 template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  if constexpr (R <= 56) {
+    if (h->fx && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) return launch_fx<R>(h, p, st);
+  }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 56) {
       if (h->kernel_variant == 3 && p.energy == nullptr) return launch_tc<R>(h, p, st);
@@ -404,6 +483,14 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
     const int ix = (x == h->d_U[0]) ? 0 : 1;
     p.x32_in = h->d_X32[ix];
     p.x32_out = h->d_X32[1 - ix];
+    if (h->fx) {
+      p.xsl_in = h->d_Xsl[ix];
+      p.xsl_out = h->d_Xsl[1 - ix];
+      p.xex_in = h->d_Xex[ix];
+      p.xex_out = h->d_Xex[1 - ix];
+      p.bsl = h->d_Bsl;
+      p.bex = h->d_Bex;
+    }
   }
   if (mode == tsp::kModeApply || mode == tsp::kModePower) p.S = 1;  // single-vector products
   p.dt_elem = h->d_dt_elem;
@@ -430,6 +517,7 @@ int refresh_shadow(tsp_handle* h, int i) {
   const int ntile = (h->S + 63) / 64;
   tsp::k_make_shadow<<<1184, 256, 0, h->stream>>>(h->d_U[i], h->d_X32[i], h->ne, h->S, h->R, ntile);
   TSP_CUDA(h, cudaGetLastError());
+  if (h->fx) return fx_dispatch(h, false, i);
   return TSP_OK;
 }
 

@@ -72,6 +72,15 @@ struct StepParams {
   const int* src_of;          // per-element source index into src_phi/F, -1 if none
   const int* mesh_of;         // per-element mesh id (power iteration per mesh)
   const double* xscale_mesh;  // per-mesh power-iteration scale
+  // Tensor-core fixed-point path: slice images of the state (per element and
+  // 64-shot tile) and of the operator (per block), with the shared binary
+  // exponents of their rows (per shot of a tile, per block row).
+  const void* xsl_in;
+  void* xsl_out;
+  const int* xex_in;
+  int* xex_out;
+  const void* bsl;
+  const int* bex;
 };
 
 // ---------------------------------------------------------------------------
