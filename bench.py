@@ -67,11 +67,18 @@ def captured_traffic(kernel, ne, nshots):
     return rec["bytes"] * ne / rec["elements"]
 
 
+# Batched FP32 step kernels by variant (tsp_get_kernel_variant), for 2Np = 42.
+KERNELS = {0: "k_step_batched32k<42>", 1: "k_step_batched32p<42,64,4>", 2: "k_step_batched32<42>",
+           4: "k_step_batched_fx<42>"}
+
+
 def bytes_per_step(ne, Np, nnzb, nshots, precision):
     """Algorithmic HBM bytes of one step: every block once, the state read
-    (u^k, u^{k-1}) and written (u^{k+1}) once per shot, minv once."""
+    (u^k, u^{k-1}) and written (u^{k+1}) once per shot, minv once. The
+    tensor-core form ("fx") stores each operator entry as three BF16
+    fixed-point slices (6 bytes)."""
     R = 2 * Np
-    bblk = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
+    bblk = {"fp64": 8, "fp32": 4, "bf16": 2, "fx": 6}[precision]
     extra = nnzb * 4 if precision == "bf16" else 0
     return nnzb * R * R * bblk + extra + nshots * 2 * ne * Np * 24 + ne * 8
 
@@ -294,7 +301,8 @@ def single_shot_forms(args):
 
 def config_dict(args, prob):
     d = {"workload": "64-shot batched DG leap-frog: 200x100 jittered squares (40,000 triangles), Dubiner N=5, "
-                     "log-normal vp, 128 receivers, FP32 blocks / FP64 state",
+                     "log-normal vp, 128 receivers, FP32 operator / FP64 state, batched kernel chosen by the "
+                     "autotuner",
          "mesh_triangles": prob.mesh.ne if prob else 40000, "N": 5, "shots_per_gpu": args.nshots,
          "precision": args.precision, "dofs_per_shot": prob.dofs_per_shot if prob else 1680000,
          "l2": "inputs larger than L2 (state 0.86 GB per level, blocks 1.1 GB)", "parallelism": f"shots x{args.gpus}"}
@@ -340,6 +348,7 @@ def main():
     prob = make_problem(args, rank, world)
     K, Wm = args.steps, max(3, args.warmup)
     sim = capi.Simulation.from_problem(prob, precision=args.precision, device=local_rank)
+    variant = sim.kernel_variant if (prob.nshots > 1 and args.precision == "fp32") else None
     dt, lmax = estimate_dt(sim)
     prepare(sim, prob, dt, K + Wm + 2)
     sim.set_seismogram_capacity(K + Wm + 2)
@@ -362,20 +371,24 @@ def main():
     value = world * prob.nshots * dofs * K / (ms / 1e3)
     ms_step = ms / K
     hbm, peak_kind = peaks()
-    algo = bytes_per_step(prob.mesh.ne, prob.Np, sim.nnzb, prob.nshots, args.precision)
+    form = "fx" if variant == 4 else args.precision
+    algo = bytes_per_step(prob.mesh.ne, prob.Np, sim.nnzb, prob.nshots, form)
     achieved = algo / (ms_step / 1e3) / 1e9
+    kernel = (KERNELS.get(variant, "batched") if variant is not None else
+              "k_step_rows<42>" if prob.nshots == 1 else "k_step_batched<42>")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
+            "dtype": ("bf16x3 fixed-point operator, f64 state" if form == "fx" else
+                      "f32" if args.precision != "fp64" else "f64"), "data": "synthetic",
             "config": config_dict(args, prob), "dt": dt, "lmax": lmax,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": (captured_traffic("k_step_batched32k<42>", prob.mesh.ne, prob.nshots)
-                                     if prob.nshots > 1 and args.precision == "fp32" else
+                         "traffic": (captured_traffic(kernel, prob.mesh.ne, prob.nshots)
+                                     if variant is not None else
                                      captured_traffic("k_step_rows<42,double>", prob.mesh.ne, prob.nshots)
                                      if prob.nshots == 1 and args.precision == "fp64" else None)
                          if prob.N == 5 else None,
                          "traffic_source": "ncu capture (profiles/traffic.json) scaled by element rows",
-                         "kernel": "k_step_batched32k<42>" if prob.nshots > 1 else "k_step_rows<42>",
+                         "kernel": kernel, "kernel_variant": variant,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_step": algo},
             "gpu_launches": K + 1, "clocks": clocks}

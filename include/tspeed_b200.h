@@ -174,6 +174,13 @@ int tsp_run(tsp_handle* h, int64_t nsteps);
  * replay; synchronises and returns the device time in milliseconds. */
 int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
 
+/* Kernel variant of the batched FP32 step chosen for this handle by the
+ * autotuner at creation (or forced by TSP_BATCHED_VARIANT): 0 K-split /
+ * pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel, 2 non-persistent
+ * CUDA-core kernel, 4 tensor-core fixed-point kernel. No counterpart in the
+ * reference (its step is a single CPU path). */
+int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant);
+
 /* Number of leap-frog steps done (first_step counts as 1) and the
  * reference's M_last_time. */
 int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time);

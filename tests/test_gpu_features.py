@@ -114,3 +114,36 @@ def test_error_codes():
     assert e.value.code == -6  # clockwise triangle
     with pytest.raises(capi.TspError):
         s.seismograms(0, 10 ** 9)
+
+
+def test_autotuner_choice_and_override(monkeypatch):
+    """The batched FP32 step is chosen by the autotuner at creation (one of
+    the CUDA-core variants 0/1/2 or the tensor-core variant 4); the chosen
+    kernel stays within the 1e-4 budget of FP64; TSP_BATCHED_VARIANT forces
+    a variant."""
+    m = W.jittered_rect(8, 5, 800.0, 500.0, seed=31)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    rng = np.random.default_rng(4)
+    shots = [(40 + 720 * rng.random(), 40 + 420 * rng.random()) for _ in range(70)]
+    rcv = W.surface_receivers(m, 4)
+    n = 80
+    seis = {}
+    monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
+    dt = None
+    for prec in ("fp64", "fp32"):
+        with capi.Simulation.create(m.xy, m.tri, 5, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
+            if prec == "fp32":
+                assert s.kernel_variant in (0, 1, 2, 4)
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
+            s.set_dt(dt)
+            for k in range(70):
+                s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
+            s.first_step()
+            s.run(n - 1)
+            seis[prec] = s.seismograms(0, n)
+    err = np.linalg.norm(seis["fp32"] - seis["fp64"]) / np.linalg.norm(seis["fp64"])
+    assert err < 1e-4, err
+    monkeypatch.setenv("TSP_BATCHED_VARIANT", "2")
+    with capi.Simulation.create(m.xy, m.tri, 5, lam, mu, rho, shots, rcv, penalty=10.0, precision="fp32") as s:
+        assert s.kernel_variant == 2

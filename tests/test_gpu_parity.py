@@ -295,36 +295,6 @@ def test_matrix_free_energy_and_resume():
         assert np.array_equal(a.u(), b.u())
 
 
-@pytest.mark.parametrize("N", [4, 5, 6])
-def test_tensor_core_batched_step(N, monkeypatch):
-    """tcgen05 BF16x3 batched step (variant 3) against the FP64 batched path
-    and the FP32 CUDA-core kernel, 70 shots (one full and one partial tile)."""
-    m = W.jittered_rect(8, 5, 800.0, 500.0, seed=N + 90)
-    rng = np.random.default_rng(N + 7)
-    vp = 2500 + 1500 * rng.random(m.ne)
-    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
-    shots = [(40 + 720 * rng.random(), 40 + 420 * rng.random()) for _ in range(70)]
-    rcv = W.surface_receivers(m, 6)
-    n = 150
-    out = {}
-    dt = None
-    for tag, prec, variant in (("fp64", "fp64", "0"), ("simt", "fp32", "0"), ("tc", "fp32", "3")):
-        monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
-        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
-            if dt is None:
-                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
-            s.set_dt(dt)
-            for k in range(70):
-                s.set_ricker(k, 25.0, 0.04, -1.0, k % 2, n)
-            s.first_step()
-            s.run(n - 1)
-            out[tag] = (s.seismograms(0, n), s.u(3), s.u(66))
-    for i in range(3):
-        assert rel(out["tc"][i], out["fp64"][i]) < 1e-4
-        assert rel(out["tc"][i], out["simt"][i]) < 1e-4
-    print("tc vs fp64:", rel(out["tc"][0], out["fp64"][0]), "simt vs fp64:", rel(out["simt"][0], out["fp64"][0]))
-
-
 @pytest.mark.parametrize("N", [2, 4, 5, 6])
 def test_fixed_point_tensor_core_step(N, monkeypatch):
     """Tensor-core step with fixed-point BF16 slices and an exact main

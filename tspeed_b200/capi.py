@@ -58,6 +58,7 @@ SIGNATURES = {
     "tsp_run": (C.c_int, [C.c_void_p, C.c_int64]),
     "tsp_run_timed": (C.c_int, [C.c_void_p, C.c_int64, _dp]),
     "tsp_get_progress": (C.c_int, [C.c_void_p, _lp, _dp]),
+    "tsp_get_kernel_variant": (C.c_int, [C.c_void_p, _ip]),
     "tsp_get_u": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "tsp_get_seismograms": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _dp]),
     "tsp_set_seismogram_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
@@ -280,6 +281,14 @@ class Simulation:
         k, t = C.c_int64(), C.c_double()
         _check(lib().tsp_get_progress(self._h, C.byref(k), C.byref(t)), self._h)
         return k.value, t.value
+
+    @property
+    def kernel_variant(self) -> int:
+        """Batched-step kernel chosen by the autotuner (or TSP_BATCHED_VARIANT):
+        0/1/2 CUDA-core kernels, 4 tensor-core fixed-point kernel."""
+        v = C.c_int32()
+        _check(lib().tsp_get_kernel_variant(self._h, C.byref(v)), self._h)
+        return v.value
 
     # ---- outputs ----
     def u(self, shot: int = 0):

@@ -53,8 +53,9 @@ struct tsp_handle {
   bool shadow = false;
   // FP32 batched step variant: 0 K split over warp groups (2Np <= 42) or the
   // pipelined single group (2Np = 56); 1 pipelined single group; 2 the
-  // non-persistent cp.async kernel. Selected by TSP_BATCHED_VARIANT.
-  int kernel_variant = 0;
+  // non-persistent cp.async kernel; 4 the tensor-core fixed-point kernel.
+  // -1 until the autotuner has chosen; TSP_BATCHED_VARIANT forces one.
+  int kernel_variant = -1;
   // Tensor-core fixed-point step (variant 4): operator slice images and row
   // scales, built once; state slice images and shot scales, one pair per
   // state level like the FP32 shadow.
@@ -212,6 +213,69 @@ int fx_dispatch(tsp_handle* h, bool setup, int i) {
   }
 }
 
+int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, double* out, int rel,
+                double xscale, cudaStream_t st);
+int check_device_error(tsp_handle* h);
+
+// Autotuner of the batched FP32 step: each applicable kernel variant (tile
+// shape, shots per CTA, CUDA cores or tensor cores) runs a few steps on the
+// zero initial state of the handle -- no sources are set yet, so every
+// output stays zero and nothing needs restoring -- timed with CUDA events on
+// the handle's stream; the fastest is kept. TSP_BATCHED_VARIANT skips it.
+int autotune(tsp_handle* h) {
+  const bool fx_ok = h->fx;
+  if (h->kernel_variant >= 0 || !h->shadow) {
+    if (h->kernel_variant < 0) h->kernel_variant = 0;
+    return TSP_OK;
+  }
+  std::vector<int> cands;
+  if (h->R <= 42) cands = {0, 1, 2};
+  else if (h->R <= 56) cands = {0, 2};
+  else cands = {2};
+  if (fx_ok) cands.push_back(4);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  TSP_CUDA(h, cudaEventCreate(&e0));
+  TSP_CUDA(h, cudaEventCreate(&e1));
+  float best = 0.0f;
+  int bestv = cands[0], rc = TSP_OK;
+  for (int v : cands) {
+    h->kernel_variant = v;
+    h->fx = (v == 4);
+    for (int w = 0; w < 2 && !rc; ++w) rc = launch_step(h, tsp::kModeStep, h->d_U[1], h->d_U[0], h->d_U[0], 0, 1.0, h->stream);
+    if (!rc) rc = cudaEventRecord(e0, h->stream) == cudaSuccess ? TSP_OK : TSP_ERR_CUDA;
+    for (int w = 0; w < 5 && !rc; ++w) rc = launch_step(h, tsp::kModeStep, h->d_U[1], h->d_U[0], h->d_U[0], 0, 1.0, h->stream);
+    if (!rc) rc = cudaEventRecord(e1, h->stream) == cudaSuccess ? TSP_OK : TSP_ERR_CUDA;
+    float ms = 0.0f;
+    if (!rc) rc = (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+                      ? TSP_OK
+                      : TSP_ERR_CUDA;
+    if (rc) break;
+    if (v == cands[0] || ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc == TSP_ERR_CUDA ? fail(h, TSP_ERR_CUDA, "autotuner launch failed") : rc;
+  if ((rc = check_device_error(h))) return rc;
+  h->kernel_variant = bestv;
+  h->fx = (bestv == 4);
+  if (fx_ok && !h->fx) {
+    dfree(h, h->d_Bsl);
+    dfree(h, h->d_Bex);
+    h->d_Bsl = nullptr;
+    h->d_Bex = nullptr;
+    for (int i = 0; i < 2; ++i) {
+      dfree(h, h->d_Xsl[i]);
+      dfree(h, h->d_Xex[i]);
+      h->d_Xsl[i] = nullptr;
+      h->d_Xex[i] = nullptr;
+    }
+  }
+  return TSP_OK;
+}
+
 // Common tail of both constructors: state, step counter, sources, receivers.
 int finish_create(tsp_handle* h) {
   int rc;
@@ -231,7 +295,10 @@ int finish_create(tsp_handle* h) {
       TSP_CUDA(h, cudaMemsetAsync(h->d_X32[i], 0, nsh * sizeof(float), h->stream));
     }
   }
-  h->fx = h->shadow && h->kernel_variant == 4 && h->op_kind == TSP_OP_EXPLICIT && h->R <= 56;
+  // The tensor-core kernel's slice buffers exist when it is forced or is a
+  // candidate of the autotuner.
+  const bool fx_ok = h->shadow && h->op_kind == TSP_OP_EXPLICIT && h->R <= 56;
+  h->fx = fx_ok && (h->kernel_variant == 4 || h->kernel_variant < 0);
   if (h->fx && (rc = fx_dispatch(h, true, 0))) return rc;
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
@@ -248,7 +315,7 @@ int finish_create(tsp_handle* h) {
   }
   if ((rc = alloc_seis(h, cap))) return rc;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  return TSP_OK;
+  return autotune(h);
 }
 
 template <int R, typename BT>
@@ -321,42 +388,19 @@ int launch_pipe(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 template <int R>
-int launch_tc(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
-  typedef tsp::TcCfg<R> CF;
-  const size_t smem = CF::smem_bytes();
-  static unsigned long long configured = 0;
-  const unsigned long long bit = 1ull << (h->device & 63);
-  if (!(configured & bit)) {
-    cudaError_t e =
-        cudaFuncSetAttribute(tsp::k_step_batched_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("tensor-core kernel smem: ") + cudaGetErrorString(e));
-    configured |= bit;
-  }
-  // Resident CTAs per SM, limited by shared memory and by tensor memory
-  // (512 columns per SM) so that no allocation ever waits.
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tsp::k_step_batched_tc<R>, CF::NT, smem);
-  per_sm = std::max(1, std::min(per_sm, 512 / CF::TCOLS));
-  const long long items = (long long)h->ne * ((h->S + CF::M - 1) / CF::M);
-  const unsigned grid = unsigned(std::min<long long>(items, (long long)per_sm * h->num_sms));
-  tsp::k_step_batched_tc<R><<<grid, CF::NT, smem, st>>>(p, h->d_err);
-  return TSP_OK;
-}
-
-template <int R>
 int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef FxDefault<R> CF;
   const size_t smem = CF::smem_bytes();
   static unsigned long long configured = 0;
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched_fx<R>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e =
+        cudaFuncSetAttribute(tsp::k_step_batched_fx<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("tensor-core kernel smem: ") + cudaGetErrorString(e));
     configured |= bit;
   }
-  // Persistent: one CTA per SM (its shared memory and, for 2Np >= 42, its
-  // 512 tensor-memory columns admit no second one).
+  // Persistent: one CTA per SM (its shared memory and tensor memory admit no
+  // second one).
   const long long items = (long long)h->ne * ((h->S + CF::M - 1) / CF::M);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
   tsp::k_step_batched_fx<R><<<grid, CF::NT, smem, st>>>(p, h->d_err);
@@ -387,11 +431,8 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
     if (h->fx && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) return launch_fx<R>(h, p, st);
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
-    if constexpr (R <= 56) {
-      if (h->kernel_variant == 3 && p.energy == nullptr) return launch_tc<R>(h, p, st);
-    }
     if constexpr (R <= 42) {
-      if (h->kernel_variant == 0 || h->kernel_variant == 3) return launch_ksplit<R>(h, p, st);
+      if (h->kernel_variant <= 0) return launch_ksplit<R>(h, p, st);
       return launch_pipe<R, 64, 4>(h, p, st);
     } else if constexpr (R <= 56) {
       return launch_pipe<R, 32, 2>(h, p, st);
@@ -1108,6 +1149,12 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return rc;
+}
+
+int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant) {
+  if (!h || !variant) return TSP_ERR_ARG;
+  *variant = h->kernel_variant;
+  return TSP_OK;
 }
 
 int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time) {
