@@ -189,6 +189,12 @@ int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time
  * length 2*ne*Np. Synchronises the handle's stream. */
 int tsp_get_u(tsp_handle* h, int32_t shot, double* out);
 
+/* TimeAdvance::u() of every shot at once: out[nshots][2*ne*Np], reference
+ * layout (the state is transposed on the device and read back in large
+ * transfers; a temporary device buffer of at most 256 MiB is used).
+ * Synchronises the handle's stream. */
+int tsp_get_u_all(tsp_handle* h, double* out);
+
 /* Receiver samples, taken after every step on the device (the arithmetic of
  * TimeAdvance::eval_receivers, TimeAdvance.cpp:68-79): out[shot][k][r][2]
  * for steps k in [k0, k0+nk). k = 0 is the sample after first_step. */

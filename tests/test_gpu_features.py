@@ -147,3 +147,21 @@ def test_autotuner_choice_and_override(monkeypatch):
     monkeypatch.setenv("TSP_BATCHED_VARIANT", "2")
     with capi.Simulation.create(m.xy, m.tri, 5, lam, mu, rho, shots, rcv, penalty=10.0, precision="fp32") as s:
         assert s.kernel_variant == 2
+
+
+def test_u_all_matches_per_shot_reads():
+    """tsp_get_u_all (device transpose, chunked read-back) returns exactly the
+    per-shot tsp_get_u vectors."""
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=8)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    shots = [(100.0 + 40 * k, 120.0 + 20 * (k % 5)) for k in range(11)]
+    with capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, shots, W.surface_receivers(m, 2), penalty=10.0,
+                                precision="fp64") as s:
+        s.set_dt(1e-4)
+        for k in range(len(shots)):
+            s.set_ricker(k, 20.0, 0.05, -1.0, k % 2, 40)
+        s.first_step()
+        s.run(20)
+        allu = s.u_all()
+        for k in range(len(shots)):
+            assert np.array_equal(allu[k], s.u(k))

@@ -295,7 +295,7 @@ def test_matrix_free_energy_and_resume():
         assert np.array_equal(a.u(), b.u())
 
 
-@pytest.mark.parametrize("N", [2, 4, 5, 6])
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6])
 def test_fixed_point_tensor_core_step(N, monkeypatch):
     """Tensor-core step with fixed-point BF16 slices and an exact main
     product (variant 4), 70 shots (one full and one partial 64-shot tile):

@@ -60,6 +60,7 @@ SIGNATURES = {
     "tsp_get_progress": (C.c_int, [C.c_void_p, _lp, _dp]),
     "tsp_get_kernel_variant": (C.c_int, [C.c_void_p, _ip]),
     "tsp_get_u": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "tsp_get_u_all": (C.c_int, [C.c_void_p, _dp]),
     "tsp_get_seismograms": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _dp]),
     "tsp_set_seismogram_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
     "tsp_enable_energy": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -294,6 +295,12 @@ class Simulation:
     def u(self, shot: int = 0):
         out = np.zeros(2 * self.ne * self.Np)
         _check(lib().tsp_get_u(self._h, shot, _d(out)), self._h)
+        return out
+
+    def u_all(self):
+        """u() of every shot: [nshots][2*ne*Np], reference layout."""
+        out = np.zeros((self.nshots, 2 * self.ne * self.Np))
+        _check(lib().tsp_get_u_all(self._h, _d(out)), self._h)
         return out
 
     def seismograms(self, k0: int, nk: int):

@@ -1169,6 +1169,21 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Shots [s0, s0+ns) of a device state u[(e*S + s)*2Np + c*Np + i] in the
+// reference's vector layout out[s - s0][c*ne*Np + e*Np + i]
+// (FESpace_imp.hpp:152-153): one thread per output value, coalesced writes.
+__global__ void k_state_to_ref(const double* __restrict__ u, int ne, int S, int Np, int s0, int ns,
+                               double* __restrict__ out) {
+  const long long per = 2ll * ne * Np;
+  const long long n = per * ns;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const long long sl = o / per, rem = o - sl * per;
+    const long long c = rem / ((long long)ne * Np), rem2 = rem - c * ne * Np;
+    const long long e = rem2 / Np, i = rem2 - e * Np;
+    out[o] = u[(e * S + s0 + sl) * 2 * Np + c * Np + i];
+  }
+}
+
 // FP32 transposed shadow of a whole FP64 state (before first_step and after
 // tsp_set_state): one thread per (element, tile, row, shot-in-tile).
 __global__ void k_make_shadow(const double* __restrict__ u, float* __restrict__ x32, int ne, int S, int R,
