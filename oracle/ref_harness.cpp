@@ -8,7 +8,9 @@
 //   * the operator B blocks (TimeAdvance_imp.hpp:32) in a merged 2Np x 2Np
 //     per (row, col) layout, with the block-CSR pattern of MyMat
 //     (MyMat.cpp:128-154),
-//   * the inverse-mass scalars (Matrices_imp.hpp:187,189),
+//   * the inverse-mass scalars (Matrices_imp.hpp:187,189) and the reference
+//     element's inverse mass matrix (FESpace_imp.hpp:48-68; the identity for
+//     the orthonormal Dubiner basis, dense for BoundaryAdapted),
 //   * the mesh neighbour tables (Mesh.cpp:33-128),
 //   * source / receiver location (Receivers_imp.hpp:34-51),
 //   * displacement snapshots and receiver samples of the leap-frog loop
@@ -18,6 +20,10 @@
 // in the LeapFrog constructor with the default M_penalty(2)
 // (TimeAdvance_imp.hpp:27,32), so set_penalty() called afterwards has no
 // effect; M_penalty, M_mat and B are protected (TimeAdvance.hpp:214-228).
+//
+// --basis ba runs the reference with FESpace<N, Dunavant<2N>,
+// BoundaryAdapted<N>>, the space of Examples/src/Lamb.cpp:26; the default is
+// FESpace<N> = FESpace<N, Gauss<N+1>, Dubiner<N>> (Examples/src/Wedge.cpp).
 //
 // Receiver samples are taken here, with the same arithmetic as
 // TimeAdvance::eval_receivers (TimeAdvance.cpp:68-79): Receivers::add
@@ -51,6 +57,7 @@ struct Args {
   bool quiet = true;
   long u_every = 0;  // snapshot interval (0: only first and last)
   bool region_mat = false;
+  bool boundary_adapted = false;
   double reg_vals[16][3];
   int reg_ids[16];
   int nreg = 0;
@@ -86,13 +93,13 @@ class LeapFrogP : public LeapFrog {
   double last_time() const { return M_last_time; }
 };
 
-template <int N>
-int run(const Args& a) {
+template <int N, typename Q, typename S>
+int run_space(const Args& a) {
   using clk = std::chrono::steady_clock;
   auto t_setup0 = clk::now();
   Mesh_ptr Th(new Mesh(a.mesh));
   const unsigned ne = Th->ne();
-  FESpace_ptr<N> Xh(new FESpace<N>(Th));
+  FESpace_ptr<N, Q, S> Xh(new FESpace<N, Q, S>(Th));
   const unsigned nln = Xh->nln();
   Parameters p(Th);
   if (a.region_mat) {
@@ -149,10 +156,12 @@ int run(const Args& a) {
       double g[5] = {t.detJ(), t.invJac()(0, 0), t.invJac()(1, 0), t.invJac()(0, 1), t.invJac()(1, 1)};
       wr(f, g, 5);
     }
-    // Inverse mass: invM blocks are I/(rho*detJ) for the orthonormal basis.
+    // Inverse mass: invM blocks are M_ref^-1/(rho*detJ) (Matrices_imp.hpp:187);
+    // the scalar 1/(rho*detJ) is their (0,0) entry over M_ref^-1(0,0).
     auto const& invM = TA.mats().getinvM();
+    const Eigen::MatrixXd minv_ref = Xh->base_invmass();
     for (unsigned e = 0; e < ne; ++e) {
-      double v = invM.component(0).elem(e)(0, 0);
+      double v = invM.component(0).elem(e)(0, 0) / minv_ref(0, 0);
       wr(f, &v, 1);
     }
     // Source location and tabulated basis (PointWiseForce via M_add).
@@ -172,6 +181,11 @@ int run(const Args& a) {
         wr(f, &v, 1);
       }
     }
+    for (unsigned i = 0; i < nln; ++i)
+      for (unsigned j = 0; j < nln; ++j) {
+        double v = minv_ref(i, j);
+        wr(f, &v, 1);
+      }
     std::fclose(f);
   }
   if (a.dump_blocks) {
@@ -248,6 +262,12 @@ int run(const Args& a) {
   return 0;
 }
 
+template <int N>
+int run(const Args& a) {
+  if (a.boundary_adapted) return run_space<N, Dunavant<2 * N>, BoundaryAdapted<N>>(a);
+  return run_space<N, Gauss<N + 1>, Dubiner<N>>(a);
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -272,6 +292,11 @@ int main(int argc, char** argv) {
     else if (k == "--sdir") a.sdir = std::atoi(nxt());
     else if (k == "--dump-blocks") a.dump_blocks = true;
     else if (k == "--u-every") a.u_every = std::atol(nxt());
+    else if (k == "--basis") {
+      const std::string b = nxt();
+      if (b == "ba") a.boundary_adapted = true;
+      else if (b != "dubiner") die("--basis must be dubiner or ba");
+    }
     else if (k == "--region") {
       // --region id lambda mu rho (repeatable): per-region setp, as the examples do.
       if (a.nreg >= 16) die("too many regions");

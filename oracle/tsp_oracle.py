@@ -30,8 +30,12 @@ import numpy as np
 # Reference element: Jacobi polynomials, Dubiner basis, Gauss rule.
 # --------------------------------------------------------------------------
 def jacobi(n: int, alpha: int, beta: int, z: np.ndarray) -> np.ndarray:
-    """Three-term recurrence of ShapeFunctions.cpp:25-60 (P_n^{alpha,beta})."""
+    """Three-term recurrence of ShapeFunctions.cpp:25-60 (P_n^{alpha,beta});
+    a negative degree gives zero there (the loop does not run on a zero
+    start, ShapeFunctions.cpp:37-39)."""
     z = np.asarray(z, dtype=np.float64)
+    if n < 0:
+        return np.zeros_like(z)
     if n == 0:
         return np.ones_like(z)
     if n == 1:
@@ -95,6 +99,77 @@ def dubiner_grad(N: int, csi, eta) -> np.ndarray:
                                         * jacobi(j - 1, 2 * i + 2, 1, 2 * eta - 1))
         out.append(g)
     return np.array(out)
+
+
+def ba_phi(N: int, csi, eta) -> np.ndarray:
+    """BoundaryAdapted<N> basis, ShapeFunctions_imp.hpp:55-118 (order: the
+    three vertex modes, the edge modes of the three families, then the
+    interior modes j outer / i inner with i + j < N). Returns [Np, npts]."""
+    csi = np.atleast_1d(np.asarray(csi, dtype=np.float64))
+    eta = np.atleast_1d(np.asarray(eta, dtype=np.float64))
+    l0 = 1 - csi - eta
+    xx = 2 * csi / (1 - eta) - 1
+    yy = 2 * eta - 1
+    out = [l0, csi.copy(), eta.copy()]
+    for i in range(1, N):
+        out.append(l0 * csi * (1 - eta) ** (i - 1) * jacobi(i - 1, 1, 1, xx))
+    for j in range(1, N):
+        out.append(l0 * eta * jacobi(j - 1, 1, 1, yy))
+    for j in range(1, N):
+        out.append(csi * eta * jacobi(j - 1, 1, 1, yy))
+    for j in range(1, N):
+        for i in range(1, N):
+            if i + j < N:
+                out.append(l0 * csi * eta * (1 - eta) ** (i - 1) * jacobi(i - 1, 1, 1, xx)
+                           * jacobi(j - 1, 2 * i + 1, 1, yy))
+    return np.array(out)
+
+
+def ba_grad(N: int, csi, eta) -> np.ndarray:
+    """Gradients of BoundaryAdapted<N>, ShapeFunctions_imp.hpp:59-116.
+    Returns [Np, npts, 2]."""
+    csi = np.atleast_1d(np.asarray(csi, dtype=np.float64))
+    eta = np.atleast_1d(np.asarray(eta, dtype=np.float64))
+    n = csi.size
+    l0 = 1 - csi - eta
+    xx = 2 * csi / (1 - eta) - 1
+    yy = 2 * eta - 1
+    out = [np.stack([-np.ones(n), -np.ones(n)], 1), np.stack([np.ones(n), np.zeros(n)], 1),
+           np.stack([np.zeros(n), np.ones(n)], 1)]
+    for i in range(1, N):
+        g0 = (1 - 2 * csi - eta) * (1 - eta) ** (i - 1) * jacobi(i - 1, 1, 1, xx) \
+            + l0 * csi * (1 - eta) ** (i - 2) * jacobi(i - 2, 2, 2, xx) * (i + 2)
+        g1 = -(1 - eta) ** (i - 2) * csi * (i + csi - i * csi - i * eta) * jacobi(i - 1, 1, 1, xx) \
+            + csi * csi * l0 * (1 - eta) ** (i - 3) * (i + 2) * jacobi(i - 2, 2, 2, xx)
+        out.append(np.stack([g0, g1], 1))
+    for j in range(1, N):
+        g0 = -eta * jacobi(j - 1, 1, 1, yy)
+        g1 = (1 - csi - 2 * eta) * jacobi(j - 1, 1, 1, yy) + l0 * eta * jacobi(j - 2, 2, 2, yy) * (j + 2)
+        out.append(np.stack([g0, g1], 1))
+    for j in range(1, N):
+        g0 = eta * jacobi(j - 1, 1, 1, yy)
+        g1 = csi * jacobi(j - 1, 1, 1, yy) + eta * csi * (j + 2) * jacobi(j - 2, 2, 2, yy)
+        out.append(np.stack([g0, g1], 1))
+    for j in range(1, N):
+        for i in range(1, N):
+            if i + j < N:
+                pa, pb = jacobi(i - 1, 1, 1, xx), jacobi(j - 1, 2 * i + 1, 1, yy)
+                g0 = eta * (1 - eta) ** (i - 2) * pb * ((1 - 2 * csi - eta) * (1 - eta) * pa
+                                                       + l0 * csi * (i + 2) * jacobi(i - 2, 2, 2, xx))
+                g1 = csi * (1 - eta) ** (i - 3) * (
+                    ((1 - eta) ** 2 * (1 - csi - 2 * eta) - (1 - eta) * eta * l0 * (i - 1)) * pa * pb
+                    + csi * l0 * eta * (i + 2) * jacobi(i - 2, 2, 2, xx) * pb
+                    + l0 * eta * (1 - eta) ** 2 * (j + 2 * i + 2) * pa * jacobi(j - 2, 2 * i + 2, 2, yy))
+                out.append(np.stack([g0, g1], 1))
+    return np.array(out)
+
+
+def basis_phi(N: int, basis: str, csi, eta) -> np.ndarray:
+    return ba_phi(N, csi, eta) if basis == "ba" else dubiner_phi(N, csi, eta)
+
+
+def basis_grad(N: int, basis: str, csi, eta) -> np.ndarray:
+    return ba_grad(N, csi, eta) if basis == "ba" else dubiner_grad(N, csi, eta)
 
 
 def gauleg(n: int, a: float, b: float):
@@ -163,7 +238,12 @@ def gauss_rule(Q: int) -> Rule:
 
 @dataclass
 class Space:
-    """Tabulated FESpace<N, Gauss<N+1>, Dubiner<N>> (FESpace_imp.hpp:25-47)."""
+    """Tabulated FESpace<N, Q, S> (FESpace_imp.hpp:25-68): S = Dubiner<N> with
+    Q = Gauss<N+1>, or S = BoundaryAdapted<N>. For BoundaryAdapted the
+    reference uses Q = Dunavant<2N> (Examples/src/Lamb.cpp:26); on affine
+    triangles every integrand is a polynomial of degree <= 2N, which the
+    collapsed Gauss<N+1> rule (degree 2N+1) also integrates exactly, so the
+    tables agree to rounding."""
     N: int
     Np: int
     rule: Rule
@@ -171,21 +251,27 @@ class Space:
     G: np.ndarray       # [Np, nq, 2] reference gradients at volume points
     Bedge: np.ndarray   # [3, Q, Np]
     Gedge: np.ndarray   # [3, Np, Q, 2]
+    basis: str = "dubiner"
+    minv_ref: np.ndarray = None  # reference inverse mass (FESpace_imp.hpp:48-68)
 
 
-def make_space(N: int) -> Space:
+def make_space(N: int, basis: str = "dubiner") -> Space:
     rule = gauss_rule(N + 1)
     Np = (N + 1) * (N + 2) // 2
     c, e = rule.nodes2d[:, 0], rule.nodes2d[:, 1]
-    B = dubiner_phi(N, c, e).T
-    G = dubiner_grad(N, c, e)
+    B = basis_phi(N, basis, c, e).T
+    G = basis_grad(N, basis, c, e)
     Bedge = np.zeros((3, N + 1, Np))
     Gedge = np.zeros((3, Np, N + 1, 2))
     for ed in range(3):
         en = rule.edge_nodes(ed)
-        Bedge[ed] = dubiner_phi(N, en[:, 0], en[:, 1]).T
-        Gedge[ed] = dubiner_grad(N, en[:, 0], en[:, 1])
-    return Space(N, Np, rule, B, G, Bedge, Gedge)
+        Bedge[ed] = basis_phi(N, basis, en[:, 0], en[:, 1]).T
+        Gedge[ed] = basis_grad(N, basis, en[:, 0], en[:, 1])
+    if basis == "ba":
+        minv_ref = np.linalg.inv(B.T @ (rule.w2d[:, None] * B))
+    else:
+        minv_ref = np.eye(Np)  # orthonormal: M_ref = I (FESpace_imp.hpp:51-54)
+    return Space(N, Np, rule, B, G, Bedge, Gedge, basis, minv_ref)
 
 
 # --------------------------------------------------------------------------
@@ -386,8 +472,8 @@ def transform(sp: Space, xy, tri, geo: Geom, fun):
     Y = p[:, 0, 1][:, None] + (p[:, 1, 1] - p[:, 0, 1])[:, None] * n2[None, :, 0] + (p[:, 2, 1] - p[:, 0, 1])[:, None] * n2[None, :, 1]
     fx, fy = fun(X, Y)
     dx = np.abs(geo.detJ)[:, None] * sp.rule.w2d[None, :]
-    rx = np.einsum("eq,qi->ei", fx * dx, sp.B)
-    ry = np.einsum("eq,qi->ei", fy * dx, sp.B)
+    rx = np.einsum("eq,qi->ei", fx * dx, sp.B) @ sp.minv_ref.T
+    ry = np.einsum("eq,qi->ei", fy * dx, sp.B) @ sp.minv_ref.T
     return np.concatenate([(rx / geo.detJ[:, None]).ravel(), (ry / geo.detJ[:, None]).ravel()])
 
 
@@ -403,7 +489,7 @@ def intriangle(xy: np.ndarray, tri: np.ndarray, e: int, px: float, py: float) ->
     return (s > -1e-6) and (t > -1e-6) and ((s + t) < (2 + 1e-6) * A)
 
 
-def locate(N: int, xy, tri, geo: Geom, px: float, py: float):
+def locate(N: int, xy, tri, geo: Geom, px: float, py: float, basis: str = "dubiner"):
     """PointWiseEntity::M_add, Receivers_imp.hpp:34-51: first element (lowest id)
     that contains the point; reference coordinates by Triangle::invmap
     (Geometry.cpp:199-202); basis values phi_s(x^)."""
@@ -414,7 +500,7 @@ def locate(N: int, xy, tri, geo: Geom, px: float, py: float):
             inv = geo.invJ[e]
             r0 = inv[0, 0] * dxp + inv[0, 1] * dyp
             r1 = inv[1, 0] * dxp + inv[1, 1] * dyp
-            return e, dubiner_phi(N, r0, r1)[:, 0]
+            return e, basis_phi(N, basis, r0, r1)[:, 0]
     raise KeyError(f"point ({px}, {py}) not found")
 
 
@@ -464,15 +550,26 @@ def apply_B(row_ptr, cols, blocks, u: np.ndarray, ne: int, Np: int) -> np.ndarra
 
 
 def leapfrog(row_ptr, cols, blocks, minv, ne, Np, dt, nsteps, src_elem, src_phi, F,
-             rcv_elems, rcv_phi, u0=None, v0=None, snap_steps=()):
+             rcv_elems, rcv_phi, u0=None, v0=None, snap_steps=(), minv_ref=None):
     """Runs first_step + (nsteps-1) step() calls. F[k] = (Fx, Fy) at the force
     time of step k. Returns (u after nsteps, seismogram [nsteps, nr, 2],
     snapshots {step: u}). Receivers are sampled after every step with the
-    arithmetic of TimeAdvance::eval_receivers (TimeAdvance.cpp:68-79)."""
+    arithmetic of TimeAdvance::eval_receivers (TimeAdvance.cpp:68-79).
+    minv_ref (non-orthonormal spaces) is the reference-element inverse mass:
+    the per-element inverse mass is then minv[e] * minv_ref, a dense Np x Np
+    block (Matrices_imp.hpp:187-189)."""
     n = 2 * ne * Np
     u0 = np.zeros(n) if u0 is None else u0
     v0 = np.zeros(n) if v0 is None else v0
-    minv_full = np.concatenate([np.repeat(minv, Np), np.repeat(minv, Np)])
+    if minv_ref is None:
+        minv_diag = np.concatenate([np.repeat(minv, Np), np.repeat(minv, Np)])
+
+        def minv_full(r):
+            return minv_diag * r
+    else:
+        def minv_full(r):
+            r = r.reshape(2, ne, Np)
+            return ((r @ minv_ref.T) * minv[None, :, None]).ravel()
 
     def fvec(k):
         f = np.zeros(n)
@@ -490,14 +587,14 @@ def leapfrog(row_ptr, cols, blocks, minv, ne, Np, dt, nsteps, src_elem, src_phi,
     seis = np.zeros((nsteps, len(rcv_elems), 2))
     snaps = {}
     Bu = apply_B(row_ptr, cols, blocks, u0, ne, Np)
-    u1 = u0 + dt * v0 - minv_full * (dt * dt / 2 * (Bu - fvec(0)))
+    u1 = u0 + dt * v0 - minv_full(dt * dt / 2 * (Bu - fvec(0)))
     uold, ucur = u0, u1
     seis[0] = sample(ucur)
     if 1 in snap_steps:
         snaps[1] = ucur.copy()
     for k in range(1, nsteps):
         Bu = apply_B(row_ptr, cols, blocks, ucur, ne, Np)
-        unew = 2 * ucur - uold + minv_full * (-dt * dt * (Bu - fvec(k)))
+        unew = 2 * ucur - uold + minv_full(-dt * dt * (Bu - fvec(k)))
         uold, ucur = ucur, unew
         seis[k] = sample(ucur)
         if (k + 1) in snap_steps:

@@ -5,7 +5,10 @@ oracle/Makefile against the project's Eigen-subset shim
 (oracle/_ref/tsp_ref_run), on small seeded meshes, and stores inputs and
 outputs as .npz. Rebuild with:
 
-    make -C oracle REF=/root/reference && python tests/golden/make_golden.py
+    make -C oracle REF=/root/reference && python tests/golden/make_golden.py [case ...]
+
+Cases named g_ba_* use the reference's BoundaryAdapted space
+(FESpace<N, Dunavant<2N>, BoundaryAdapted<N>>, Examples/src/Lamb.cpp:26).
 """
 from __future__ import annotations
 
@@ -37,6 +40,10 @@ CASES = {
                         src=(150.0, 140.0), ricker=(10.0, 0.1, 1.0, 0), nrcv=3, blocks=True),
     "g_n8": dict(nx=3, ny=2, Lx=300.0, Ly=200.0, N=8, mat="lognormal", penalty=10.0, dt=2e-5, nsteps=20,
                  src=(140.0, 90.0), ricker=(20.0, 0.05, -1.0, 1), nrcv=2, blocks=False),
+    "g_ba_n3": dict(nx=5, ny=4, Lx=500.0, Ly=400.0, N=3, mat="lognormal", penalty=10.0, dt=2e-4, nsteps=60,
+                    src=(260.0, 210.0), ricker=(50.0, 0.01, -1.0, 1), nrcv=4, blocks=True, basis="ba"),
+    "g_ba_n5": dict(nx=4, ny=3, Lx=400.0, Ly=300.0, N=5, mat="layers", penalty=10.0, dt=5e-5, nsteps=40,
+                    src=(190.0, 160.0), ricker=(150.0, 0.0015, -1.0, 0), nrcv=3, blocks=True, basis="ba"),
 }
 
 
@@ -69,6 +76,8 @@ def run_case(name, c, tmp):
            repr(t0), repr(amp), "--sdir", str(sdir), "--penalty", repr(c["penalty"])]
     if c["blocks"]:
         cmd.append("--dump-blocks")
+    if c.get("basis", "dubiner") != "dubiner":
+        cmd += ["--basis", c["basis"]]
     info = json.loads(subprocess.run(cmd, check=True, capture_output=True, text=True).stdout)
     ne = m.ne
     raw = open(out + ".mesh.bin", "rb").read()
@@ -85,6 +94,7 @@ def run_case(name, c, tmp):
     for _ in range(nr):
         rcv_elem.append(int(np.frombuffer(raw, np.int32, 1, off)[0])); off += 4
         rcv_phi.append(np.frombuffer(raw, np.float64, Np, off)); off += Np * 8
+    minv_ref = np.frombuffer(raw, np.float64, Np * Np, off).reshape(Np, Np); off += Np * Np * 8
     u = open(out + ".u.bin", "rb").read()
     rec = 8 + 16 * ne * Np
     snaps = {int(np.frombuffer(u, np.int64, 1, i)[0]): np.frombuffer(u, np.float64, 2 * ne * Np, i + 8)
@@ -95,6 +105,9 @@ def run_case(name, c, tmp):
              rcv=np.array(rcv), neigh=nb[:, :3], nedge=nb[:, 3:], detJ=geo[:, 0], minv=minv, src_elem=src_elem,
              src_phi=src_phi, rcv_elem=np.array(rcv_elem), rcv_phi=np.array(rcv_phi), seis=seis,
              u_first=snaps[1], u_final=snaps[c["nsteps"]], last_time=info["last_time"])
+    if c.get("basis", "dubiner") != "dubiner":
+        d["basis"] = c["basis"]
+        d["minv_ref"] = minv_ref
     if c["blocks"]:
         b = open(out + ".blocks.bin", "rb").read()
         h = np.frombuffer(b, np.int32, 3, 0)
@@ -110,9 +123,11 @@ def run_case(name, c, tmp):
 def main():
     if not os.path.exists(REF):
         sys.exit(f"{REF} missing: run `make -C oracle REF=/root/reference` first")
+    only = sys.argv[1:]
     with tempfile.TemporaryDirectory() as tmp:
         for name, c in CASES.items():
-            run_case(name, c, tmp)
+            if not only or name in only:
+                run_case(name, c, tmp)
 
 
 if __name__ == "__main__":

@@ -14,7 +14,10 @@ def test_neighbours_match_reference(golden):
 def test_geometry_and_minv(golden):
     o = oracle_setup(golden)
     assert np.array_equal(o["geo"].detJ, golden["detJ"])
-    assert np.max(np.abs(o["minv"] - golden["minv"]) / np.abs(golden["minv"])) == 0.0
+    # BoundaryAdapted: the reference stores 1/(rho detJ) * M_ref^-1 and the
+    # golden scalar is recovered by one division, hence one rounding.
+    tol = 0.0 if o["basis"] == "dubiner" else 4e-16
+    assert np.max(np.abs(o["minv"] - golden["minv"]) / np.abs(golden["minv"])) <= tol
 
 
 def test_points_match_reference(golden):
@@ -36,12 +39,23 @@ def test_blocks_match_reference(golden):
     assert np.abs(o["blocks"] - golden["blocks"]).max() / scale < 1e-14
 
 
+def test_reference_inverse_mass(golden):
+    """M_ref^-1 of the space (FESpace_imp.hpp:48-68): identity for Dubiner,
+    dense for BoundaryAdapted, against the matrix the reference inverted."""
+    o = oracle_setup(golden)
+    if o["basis"] == "dubiner":
+        assert np.array_equal(o["sp"].minv_ref, np.eye(o["sp"].Np))
+        return
+    ref = golden["minv_ref"]
+    assert np.abs(o["sp"].minv_ref - ref).max() / np.abs(ref).max() < 1e-12
+
+
 def test_leapfrog_matches_reference(golden):
     o = oracle_setup(golden)
     ne, Np = golden["tri"].shape[0], o["sp"].Np
     u, seis, snaps = O.leapfrog(o["row_ptr"], o["cols"], o["blocks"], o["minv"], ne, Np, float(golden["dt"]),
                                 int(golden["nsteps"]), o["src_elem"], o["src_phi"], o["F"], o["rcv_elem"],
-                                o["rcv_phi"], snap_steps=(1,))
+                                o["rcv_phi"], snap_steps=(1,), minv_ref=o["minv_ref"])
     assert rel(snaps[1], golden["u_first"]) < 1e-13
     assert rel(u, golden["u_final"]) < 1e-12
     assert np.array_equal(np.isnan(seis), np.isnan(golden["seis"]))
@@ -66,3 +80,38 @@ def test_gauleg_integrates_polynomials(n):
 def test_force_times_accumulate_like_reference():
     ts = O.force_times(1e-3, 5)
     assert ts[0] == 0.0 and ts[1] == 1e-3 + 1e-3 and ts[2] == (1e-3 + 1e-3) + 1e-3
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 5, 8])
+def test_boundary_adapted_spans_dubiner_space(N):
+    """BoundaryAdapted<N> and Dubiner<N> span the same polynomial space P_N:
+    the change of basis C (phi_BA = C phi_Dub) is exact on random points and
+    its gradients follow from the same C (ShapeFunctions_imp.hpp:55-118)."""
+    rng = np.random.default_rng(N)
+    c = rng.random(200)
+    e = rng.random(200) * (1 - c)
+    D, A = O.dubiner_phi(N, c, e), O.ba_phi(N, c, e)
+    C = np.linalg.lstsq(D.T, A.T, rcond=None)[0].T
+    assert np.abs(C @ D - A).max() < 1e-11
+    assert np.linalg.matrix_rank(C) == D.shape[0]
+    gD, gA = O.dubiner_grad(N, c, e), O.ba_grad(N, c, e)
+    assert np.abs(np.einsum("ij,jqk->iqk", C, gD) - gA).max() < 1e-9
+
+
+def test_boundary_adapted_vertex_and_edge_modes_vanish():
+    """Vertex modes are the barycentric coordinates; each edge mode vanishes
+    on the two edges it does not belong to (boundary adaptation)."""
+    N = 5
+    t = np.linspace(0.05, 0.95, 7)
+    A_e0 = O.ba_phi(N, t, 0 * t)         # edge eta = 0
+    A_e1 = O.ba_phi(N, 0 * t, t)         # edge csi = 0
+    A_e2 = O.ba_phi(N, t, 1 - t)         # edge csi + eta = 1
+    fa = slice(3, 3 + N - 1)             # family A: on eta = 0
+    fb = slice(3 + N - 1, 3 + 2 * (N - 1))   # family B: on csi = 0
+    fc = slice(3 + 2 * (N - 1), 3 + 3 * (N - 1))  # family C: on csi + eta = 1
+    interior = slice(3 + 3 * (N - 1), None)
+    assert np.abs(A_e1[fa]).max() < 1e-14 and np.abs(A_e2[fa]).max() < 1e-14
+    assert np.abs(A_e0[fb]).max() < 1e-14 and np.abs(A_e2[fb]).max() < 1e-14
+    assert np.abs(A_e0[fc]).max() < 1e-14 and np.abs(A_e1[fc]).max() < 1e-14
+    for E in (A_e0, A_e1, A_e2):
+        assert np.abs(E[interior]).max() < 1e-14
