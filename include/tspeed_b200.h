@@ -64,6 +64,20 @@ typedef enum {
   TSP_OP_MATRIX_FREE = 1  /* blocks rebuilt on the fly from reference-element matrices */
 } tsp_operator_kind;
 
+/* Modal basis of the space (ShapeFunctions.hpp): the orthonormal Dubiner<N>
+ * (FESpace<N> default) or the non-orthonormal BoundaryAdapted<N>
+ * (FESpace<N, Dunavant<2N>, BoundaryAdapted<N>>, Examples/src/Lamb.cpp:26),
+ * whose reference mass M_ref = L L^T is dense; the per-element inverse mass
+ * is then M_ref^-1 / (rho_e detJ_e) (Matrices_imp.hpp:187-189). The device
+ * advances w = L^T u with the operator L^-1 B L^-T, where the mass is again
+ * diagonal, so every kernel and precision runs unchanged; every host vector
+ * in and out of the library stays in the reference's coefficients u. Both
+ * bases span P_N. */
+typedef enum {
+  TSP_BASIS_DUBINER = 0,
+  TSP_BASIS_BOUNDARY_ADAPTED = 1
+} tsp_basis;
+
 /*
  * A simulation set up as the reference does it: mesh (Mesh.hpp:47), degree N
  * of FESpace<N> with the default Gauss<N+1> rule and Dubiner<N> basis
@@ -78,7 +92,7 @@ typedef struct {
   const double* xy;       /* [nverts][2] */
   int32_t ne;
   const int32_t* tri;     /* [ne][3] 0-based vertex ids, counter-clockwise */
-  int32_t N;              /* Dubiner degree, 1..8 */
+  int32_t N;              /* polynomial degree, 1..8 */
   const double* lambda;   /* [ne] */
   const double* mu;       /* [ne] */
   const double* rho;      /* [ne] */
@@ -90,6 +104,9 @@ typedef struct {
   int32_t nrcv;           /* >= 0 */
   const double* rcv_xy;   /* [nrcv][2] receiver points */
   int32_t device;         /* CUDA device ordinal */
+  int32_t basis;          /* tsp_basis; 0 (Dubiner) when zero-initialised.
+                             BoundaryAdapted: explicit operator only (no
+                             matrix-free operator, no multi-mesh batches) */
 } tsp_problem;
 
 /*
@@ -115,6 +132,10 @@ typedef struct {
   const int32_t* rcv_elem; /* [nrcv] */
   const double* rcv_phi;   /* [nrcv][Np] */
   int32_t device;
+  /* NULL for an orthonormal basis. Else the reference inverse mass
+   * M_ref^-1 [Np][Np] (FESpace::base_invmass, FESpace.hpp:163): the inverse
+   * mass of element e is minv[e] * M_ref^-1 (Matrices_imp.hpp:187-189). */
+  const double* ref_invmass;
 } tsp_block_problem;
 
 /* Library version and build information ("tspeed_b200 <ver> sm_100a"). */
@@ -239,9 +260,16 @@ int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax);
  * cudaMalloc/cudaFree. */
 int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* lmax);
 
-/* Exports of the assembled operator (explicit FP64 handles only):
- * row_ptr[ne+1], col[nnzb], blocks[nnzb][2Np][2Np] row-major, minv[ne]. */
+/* Exports of the assembled operator (explicit handles):
+ * row_ptr[ne+1], col[nnzb], blocks[nnzb][2Np][2Np] row-major, minv[ne].
+ * Blocks are B as the reference assembles it; for BoundaryAdapted they are
+ * recovered as L (L^-1 B L^-T) L^T from the stored operator. */
 int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* blocks, double* minv);
+
+/* Basis of the handle (tsp_basis) and its reference inverse mass M_ref^-1
+ * [Np][Np] (FESpace::base_invmass; the identity for Dubiner). Either output
+ * may be NULL. */
+int tsp_get_ref_invmass(const tsp_handle* h, int32_t* basis, double* out);
 
 /* Source and receiver location: elements and basis values. */
 int tsp_export_points(tsp_handle* h, int32_t* src_elem, double* src_phi, int32_t* rcv_elem, double* rcv_phi);
@@ -282,6 +310,10 @@ int tsp_batch_get_seismograms(tsp_batch* b, int32_t mesh, int64_t k0, int64_t nk
 int tsp_quadrature_points(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, double* pts);
 int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
                 double* out);
+/* The same for a given basis (tsp_basis): uh = M_ref^-1 rhs / detJ
+ * (FESpace_imp.hpp:152-153). tsp_project is this with TSP_BASIS_DUBINER. */
+int tsp_project_basis(int32_t N, int32_t basis, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri,
+                      const double* fvals, double* out);
 
 /* Host-side mesh services (Mesh.cpp). */
 /* Gmsh 2.2 ASCII reader (Mesh::Mesh, Mesh.cpp:174-257): counts first

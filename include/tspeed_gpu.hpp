@@ -90,11 +90,15 @@ class Mesh {
 typedef std::shared_ptr<Mesh> Mesh_ptr;
 
 // FESpace<N, Gauss<N+1>, Dubiner<N>> (FESpace.hpp:37-180).
+// FESpace<N> (Dubiner<N>, the reference default) or, with
+// TSP_BASIS_BOUNDARY_ADAPTED, FESpace<N, Dunavant<2N>, BoundaryAdapted<N>>
+// (Examples/src/Lamb.cpp:26).
 class FESpace {
  public:
-  FESpace(Mesh_ptr m, int N) : mesh_(std::move(m)), N_(N) {
+  FESpace(Mesh_ptr m, int N, tsp_basis basis = TSP_BASIS_DUBINER) : mesh_(std::move(m)), N_(N), basis_(basis) {
     if (N < 1 || N > 8) throw Error(TSP_ERR_UNSUPPORTED, "degree N must be in 1..8");
   }
+  tsp_basis basis() const { return basis_; }
   Mesh_ptr mesh() const { return mesh_; }
   int degree() const { return N_; }
   unsigned nln() const { return unsigned((N_ + 1) * (N_ + 2) / 2); }
@@ -110,14 +114,15 @@ class FESpace {
       vals[2 * q] = f[0];
       vals[2 * q + 1] = f[1];
     }
-    check(tsp_project(N_, int32_t(mesh_->nverts()), mesh_->xy().data(), ne, mesh_->tri().data(), vals.data(),
-                      out.data()));
+    check(tsp_project_basis(N_, basis_, int32_t(mesh_->nverts()), mesh_->xy().data(), ne, mesh_->tri().data(),
+                            vals.data(), out.data()));
     return out;
   }
 
  private:
   Mesh_ptr mesh_;
   int N_;
+  tsp_basis basis_;
 };
 typedef std::shared_ptr<FESpace> FESpace_ptr;
 
@@ -292,6 +297,7 @@ class LeapFrog {
     P.nrcv = int32_t(rcv_.size());
     P.rcv_xy = rxy.empty() ? nullptr : rxy.data();
     P.device = device_;
+    P.basis = Xh_->basis();
     check(tsp_create(&P, &h_));
     check(tsp_set_dt(h_, dt_), h_);
     // Force table over the run (time accumulation of TimeAdvance.cpp:46).

@@ -12,10 +12,23 @@ from tspeed_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
+def basis_of(g):
+    return str(g["basis"]) if "basis" in g else "dubiner"
+
+
+# Relative tolerances of the FP64 paths against the reference: 1e-12 for the
+# orthonormal Dubiner basis; the dense M_ref^-1 of BoundaryAdapted amplifies
+# rounding by its condition number (1.3e4 at N = 3, 1.1e5 at N = 5), so the
+# BoundaryAdapted cases are held to 1e-11 (u after the first step: 1e-13 and
+# 1e-12).
+def tols(g):
+    return (1e-13, 1e-12) if basis_of(g) == "dubiner" else (1e-12, 1e-11)
+
+
 def sim_from_golden(g, precision="fp64", shots=None):
     src = [tuple(g["src"])] if shots is None else shots
     s = capi.Simulation.create(g["xy"], g["tri"], int(g["N"]), g["lam"], g["mu"], g["rho"], src, g["rcv"],
-                               penalty=float(g["penalty"]), precision=precision)
+                               penalty=float(g["penalty"]), precision=precision, basis=basis_of(g))
     s.set_dt(float(g["dt"]))
     f0, t0, amp, sdir = g["ricker"]
     for k in range(s.nshots):
@@ -38,9 +51,11 @@ def test_golden_run_through_device_assembly(golden):
         u = s.u()
         seis = s.seismograms(0, int(g["nsteps"]))[0]
         k, t = s.progress()
-    assert rel(u1, g["u_first"]) < 1e-13
-    assert rel(u, g["u_final"]) < 1e-12
-    assert finite_rel(seis, g["seis"]) < 1e-12
+    t1, tn = tols(g)
+    print(g["name"], "u1", rel(u1, g["u_first"]), "u", rel(u, g["u_final"]), "seis", finite_rel(seis, g["seis"]))
+    assert rel(u1, g["u_first"]) < t1
+    assert rel(u, g["u_final"]) < tn
+    assert finite_rel(seis, g["seis"]) < tn
     # The product evaluates the basis at the collapsed vertex by its limit
     # where the reference yields NaN.
     assert np.isfinite(seis).all()
@@ -55,8 +70,18 @@ def test_golden_operator_export(golden):
         se, sp, re_, rp = s.export_points()
     assert np.array_equal(row_ptr, o["row_ptr"]) and np.array_equal(col, o["cols"])
     ref = g["blocks"] if "blocks" in g else o["blocks"]
-    assert np.abs(blocks - ref).max() / np.abs(ref).max() < 1e-13
-    assert np.array_equal(minv, g["minv"])
+    t1, _ = tols(g)
+    # BoundaryAdapted blocks come back as M_ref (M_ref^-1 B) from the stored
+    # product; the golden minv of that case is recovered by one division.
+    print(g["name"], "blocks", np.abs(blocks - ref).max() / np.abs(ref).max())
+    assert np.abs(blocks - ref).max() / np.abs(ref).max() < t1
+    if basis_of(g) == "dubiner":
+        assert np.array_equal(minv, g["minv"])
+    else:
+        assert np.abs(minv - g["minv"]).max() / np.abs(g["minv"]).max() <= 4e-16
+        with sim_from_golden(g) as s:
+            assert s.basis == "ba"
+            assert np.abs(s.ref_invmass() - g["minv_ref"]).max() / np.abs(g["minv_ref"]).max() < 1e-12
     assert se[0] == int(g["src_elem"]) and list(re_) == list(g["rcv_elem"])
     assert np.allclose(sp[0], g["src_phi"], rtol=0, atol=1e-13)
     ok = np.isfinite(g["rcv_phi"])
@@ -71,7 +96,8 @@ def test_golden_run_from_reference_blocks(golden):
     rphi = np.nan_to_num(g["rcv_phi"])
     f0, t0, amp, sdir = g["ricker"]
     with capi.Simulation.from_blocks(g["row_ptr"], g["col"], g["blocks"], g["minv"], [int(g["src_elem"])],
-                                     g["src_phi"][None], g["rcv_elem"], rphi) as s:
+                                     g["src_phi"][None], g["rcv_elem"], rphi,
+                                     ref_invmass=g["minv_ref"] if "minv_ref" in g else None) as s:
         s.set_dt(float(g["dt"]))
         s.set_ricker(0, f0, t0, amp, int(sdir), int(g["nsteps"]))
         s.first_step()
@@ -79,8 +105,10 @@ def test_golden_run_from_reference_blocks(golden):
             s.step()
         u = s.u()
         seis = s.seismograms(0, int(g["nsteps"]))[0]
-    assert rel(u, g["u_final"]) < 1e-12
-    assert finite_rel(seis, g["seis"]) < 1e-12
+    _, tn = tols(g)
+    print(g["name"], "from blocks: u", rel(u, g["u_final"]), "seis", finite_rel(seis, g["seis"]))
+    assert rel(u, g["u_final"]) < tn
+    assert finite_rel(seis, g["seis"]) < tn
 
 
 @pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7, 8])
@@ -243,6 +271,8 @@ def test_fp32_batched_pipeline_multi_tile(N):
 def test_golden_run_matrix_free(golden):
     """The matrix-free operator (no stored blocks) against the reference run."""
     g = golden
+    if basis_of(g) != "dubiner":
+        pytest.skip("the matrix-free operator is built for the Dubiner basis")
     s = capi.Simulation.create(g["xy"], g["tri"], int(g["N"]), g["lam"], g["mu"], g["rho"], [tuple(g["src"])],
                                g["rcv"], penalty=float(g["penalty"]), op="matrix_free")
     with s:
@@ -363,3 +393,124 @@ def test_fixed_point_tensor_core_resume_and_energy(monkeypatch):
         drift[variant] = np.max(np.abs(E - E[0])) / E[0]
     print("energy drift: simt", drift["0"], "fx", drift["4"])
     assert drift["4"] < 1e-5
+
+
+def _ba_problem(N, seed):
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=seed)
+    rng = np.random.default_rng(seed)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    shots = [(40 + 520 * rng.random(), 40 + 320 * rng.random()) for _ in range(5)]
+    return m, lam, mu, rho, shots, W.surface_receivers(m, 5)
+
+
+@pytest.mark.parametrize("N", [1, 3, 5, 8])
+def test_boundary_adapted_apply_matches_oracle(N):
+    """B x through the product (stored M_ref^-1 B, returned as B x) against
+    the oracle's BoundaryAdapted assembly, and the reference inverse mass."""
+    m, lam, mu, rho, _, _ = _ba_problem(N, 40 + N)
+    sp = O.make_space(N, "ba")
+    tri = m.tri.astype(np.int64)
+    geo = O.geometry(m.xy, tri)
+    nb, ned = O.neighbours(tri)
+    row_ptr, cols, blocks, minv = O.assemble(sp, geo, nb, ned, lam, mu, rho, 10.0)
+    x = np.random.default_rng(N).standard_normal(2 * m.ne * sp.Np)
+    y_ref = O.apply_B(row_ptr, cols, blocks, x, m.ne, sp.Np)
+    with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, [(250.0, 200.0)], [], penalty=10.0, basis="ba") as s:
+        y = s.apply(x)
+        mi = s.ref_invmass()
+    print("N", N, "apply", rel(y, y_ref))
+    assert rel(y, y_ref) < 1e-11
+    assert np.abs(mi - sp.minv_ref).max() / np.abs(sp.minv_ref).max() < 1e-12
+
+
+@pytest.mark.parametrize("N", [2, 5])
+def test_boundary_adapted_matches_dubiner_seismograms(N):
+    """Both bases span P_N and every form is integrated exactly, so the
+    seismograms of five shots agree up to rounding; so do the discrete
+    energy and the spectrum of M^-1 B, which do not depend on the basis."""
+    m, lam, mu, rho, shots, rcv = _ba_problem(N, 50 + N)
+    n = 150
+    out, lmax, en = {}, {}, {}
+    dt = None
+    for basis in ("dubiner", "ba"):
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0, basis=basis) as s:
+            lmax[basis] = s.estimate_lmax(300)
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(lmax[basis])
+            s.set_dt(dt)
+            for k in range(len(shots)):
+                s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
+            s.set_seismogram_capacity(n)
+            s.enable_energy(True)
+            s.first_step()
+            s.run(n - 1)
+            out[basis] = s.seismograms(0, n)
+            en[basis] = s.energy(1, n - 1)
+    print("N", N, "seis", rel(out["ba"], out["dubiner"]), "energy", rel(en["ba"], en["dubiner"]), "lmax", lmax)
+    assert (np.abs(out["dubiner"][:, -1]) > 0).any()
+    assert rel(out["ba"], out["dubiner"]) < 1e-10
+    assert np.abs(en["dubiner"]).max() > 0 and rel(en["ba"], en["dubiner"]) < 1e-10
+    assert abs(lmax["ba"] - lmax["dubiner"]) < 1e-2 * lmax["dubiner"]
+
+
+def test_boundary_adapted_fp32_batched_close_to_fp64(monkeypatch):
+    """The orthonormalised BoundaryAdapted operator L^-1 B L^-T through the
+    FP32 multi-shot kernels (the autotuner's choice, and the tensor-core
+    kernel forced), within the 1e-4 seismogram budget of the FP64
+    BoundaryAdapted run."""
+    m, lam, mu, rho, shots, rcv = _ba_problem(4, 61)
+    n = 150
+    out = {}
+    dt = None
+    for key, prec, variant in (("fp64", "fp64", None), ("auto", "fp32", None), ("fx", "fp32", "4")):
+        if variant:
+            monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+        else:
+            monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
+        with capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec,
+                                    basis="ba") as s:
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(100))
+            s.set_dt(dt)
+            for k in range(len(shots)):
+                s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
+            s.first_step()
+            s.run(n - 1)
+            out[key] = s.seismograms(0, n)
+            if key == "fx":
+                assert s.kernel_variant == 4
+    for key in ("auto", "fx"):
+        print(key, rel(out[key], out["fp64"]))
+        assert rel(out[key], out["fp64"]) < 1e-4
+
+
+def test_boundary_adapted_checkpoint_resume_and_initial_state():
+    """States cross the boundary in the reference's coefficients u while the
+    device holds w = L^T u: a checkpoint taken and restored continues the run
+    to rounding, and a projected initial field read back before any step is
+    the field that went in."""
+    m, lam, mu, rho, shots, rcv = _ba_problem(3, 71)
+    n = 120
+    mk = lambda: capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, shots[:2], rcv,  # noqa: E731
+                                        penalty=10.0, basis="ba")
+    pts = capi.quadrature_points(3, m.xy, m.tri)
+    fx = np.exp(-((pts[..., 0] - 300.0) ** 2 + (pts[..., 1] - 200.0) ** 2) / 80.0 ** 2) * 1e-6
+    u0 = capi.project(3, m.xy, m.tri, np.stack([fx, 0.5 * fx], -1), basis="ba")
+    with mk() as a, mk() as b:
+        dt = 0.4 * 2 / np.sqrt(a.estimate_lmax(100))
+        for s in (a, b):
+            s.set_dt(dt)
+            for k in range(2):
+                s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
+        a.set_initial(0, u0, None)
+        assert rel(a.u(0), u0) < 1e-14
+        a.first_step()
+        a.run(40)
+        b.set_state(*a.get_state())
+        a.run(n - 42)
+        b.run(n - 42)
+        print("resume", rel(b.u(0), a.u(0)), rel(b.u(1), a.u(1)))
+        assert rel(b.u(0), a.u(0)) < 1e-12 and rel(b.u(1), a.u(1)) < 1e-12
+        assert rel(b.u_all(), a.u_all()) < 1e-12
+        assert rel(a.u_all()[1], a.u(1)) < 1e-15  # device and host maps, same L^-T

@@ -115,3 +115,31 @@ def test_boundary_adapted_vertex_and_edge_modes_vanish():
     assert np.abs(A_e0[fc]).max() < 1e-14 and np.abs(A_e1[fc]).max() < 1e-14
     for E in (A_e0, A_e1, A_e2):
         assert np.abs(E[interior]).max() < 1e-14
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_seismograms_do_not_depend_on_the_basis(N):
+    """Dubiner<N> and BoundaryAdapted<N> span the same space and the SIPG
+    forms are integrated exactly, so the discrete solution, sampled at the
+    receivers, is the same function; only the rounding differs."""
+    from tspeed_b200 import workloads as W
+    m = W.jittered_rect(5, 4, 500.0, 400.0, seed=3)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1750.0), np.full(m.ne, 2100.0))
+    tri = m.tri.astype(np.int64)
+    geo = O.geometry(m.xy, tri)
+    nb, ned = O.neighbours(tri)
+    rcv = W.surface_receivers(m, 4)
+    dt, n = 2e-4, 150
+    F = [(0.0, O.ricker(t, 80.0, 0.0125, -1.0)) for t in O.force_times(dt, n)]
+    out = {}
+    for basis in ("dubiner", "ba"):
+        sp = O.make_space(N, basis)
+        row_ptr, cols, blocks, minv = O.assemble(sp, geo, nb, ned, lam, mu, rho, 10.0)
+        se, sphi = O.locate(N, m.xy, tri, geo, 255.0, 205.0, basis=basis)
+        rl = [O.locate(N, m.xy, tri, geo, x, y, basis=basis) for (x, y) in rcv]
+        _, seis, _ = O.leapfrog(row_ptr, cols, blocks, minv, m.ne, sp.Np, dt, n, se, sphi, F,
+                                [r[0] for r in rl], [r[1] for r in rl],
+                                minv_ref=None if basis == "dubiner" else sp.minv_ref)
+        out[basis] = seis
+    assert (np.abs(out["dubiner"][-1]) > 0).all()
+    assert rel(out["ba"], out["dubiner"]) < 1e-12

@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(_HERE, "libtspeed_b200.so")
 
 TSP_PREC = {"fp64": 0, "fp32": 1, "bf16": 2}
 TSP_OP = {"explicit": 0, "matrix_free": 1}
+# Modal basis: Dubiner<N> (orthonormal) or BoundaryAdapted<N> (ShapeFunctions.hpp).
+TSP_BASIS = {"dubiner": 0, "ba": 1, "boundary_adapted": 1}
 STATUS = {0: "TSP_OK", -1: "TSP_ERR_ARG", -2: "TSP_ERR_CUDA", -3: "TSP_ERR_NOMEM", -4: "TSP_ERR_STATE",
           -5: "TSP_ERR_NOT_FOUND", -6: "TSP_ERR_MESH", -7: "TSP_ERR_NONFINITE", -8: "TSP_ERR_TIMEOUT",
           -9: "TSP_ERR_UNSUPPORTED"}
@@ -30,14 +32,14 @@ class TspProblem(C.Structure):
     _fields_ = [("nverts", C.c_int32), ("xy", _dp), ("ne", C.c_int32), ("tri", _ip), ("N", C.c_int32),
                 ("lambda_", _dp), ("mu", _dp), ("rho", _dp), ("penalty", C.c_double), ("precision", C.c_int32),
                 ("op_kind", C.c_int32), ("nshots", C.c_int32), ("src_xy", _dp), ("nrcv", C.c_int32),
-                ("rcv_xy", _dp), ("device", C.c_int32)]
+                ("rcv_xy", _dp), ("device", C.c_int32), ("basis", C.c_int32)]
 
 
 class TspBlockProblem(C.Structure):
     _fields_ = [("ne", C.c_int32), ("Np", C.c_int32), ("nnzb", C.c_int32), ("row_ptr", _ip), ("col", _ip),
                 ("blocks", _dp), ("minv", _dp), ("precision", C.c_int32), ("nshots", C.c_int32),
                 ("src_elem", _ip), ("src_phi", _dp), ("nrcv", C.c_int32), ("rcv_elem", _ip), ("rcv_phi", _dp),
-                ("device", C.c_int32)]
+                ("device", C.c_int32), ("ref_invmass", _dp)]
 
 
 # Every symbol the header declares, with its ctypes signature.
@@ -88,6 +90,8 @@ SIGNATURES = {
     "tsp_batch_get_seismograms": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, _dp]),
     "tsp_quadrature_points": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp]),
     "tsp_project": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
+    "tsp_project_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
+    "tsp_get_ref_invmass": (C.c_int, [C.c_void_p, _ip, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
     "tsp_mesh_neighbours": (C.c_int, [C.c_int32, _ip, _ip, _ip]),
 }
@@ -163,12 +167,13 @@ def quadrature_points(N: int, xy, tri):
     return pts
 
 
-def project(N: int, xy, tri, fvals):
+def project(N: int, xy, tri, fvals, basis: str = "dubiner"):
     """FESpace::transform of a field sampled at quadrature_points()."""
     xy, tri, fvals = _f64(xy), _i32(tri), _f64(fvals)
     Np = (N + 1) * (N + 2) // 2
     out = np.zeros(2 * tri.shape[0] * Np)
-    _check(lib().tsp_project(N, xy.shape[0], _d(xy), tri.shape[0], _i(tri), _d(fvals), _d(out)))
+    _check(lib().tsp_project_basis(N, TSP_BASIS[basis], xy.shape[0], _d(xy), tri.shape[0], _i(tri), _d(fvals),
+                                   _d(out)))
     return out
 
 
@@ -194,14 +199,14 @@ class Simulation:
     # ---- construction ----
     @classmethod
     def create(cls, xy, tri, N, lam, mu, rho, src_xy, rcv_xy, penalty=2.0, precision="fp64", op="explicit",
-               device=0):
+               device=0, basis="dubiner"):
         xy, tri = _f64(xy), _i32(tri)
         lam, mu, rho = _f64(lam), _f64(mu), _f64(rho)
         src = _f64(np.asarray(src_xy, dtype=np.float64).reshape(-1, 2))
         rcv = _f64(np.asarray(rcv_xy, dtype=np.float64).reshape(-1, 2))
         p = TspProblem(xy.shape[0], _d(xy), tri.shape[0], _i(tri), N, _d(lam), _d(mu), _d(rho), penalty,
                        TSP_PREC[precision], TSP_OP[op], src.shape[0], _d(src), rcv.shape[0],
-                       _d(rcv) if rcv.shape[0] else None, device)
+                       _d(rcv) if rcv.shape[0] else None, device, TSP_BASIS[basis])
         h = C.c_void_p()
         _check(lib().tsp_create(C.byref(p), C.byref(h)))
         return cls(h)
@@ -210,11 +215,14 @@ class Simulation:
     def from_problem(cls, prob, precision="fp64", op="explicit", device=0):
         return cls.create(prob.mesh.xy, prob.mesh.tri, prob.N, prob.lam, prob.mu, prob.rho,
                           [(s.x, s.y) for s in prob.sources], prob.receivers, penalty=prob.penalty,
-                          precision=precision, op=op, device=device)
+                          precision=precision, op=op, device=device, basis=getattr(prob, "basis", "dubiner"))
 
     @classmethod
     def from_blocks(cls, row_ptr, col, blocks, minv, src_elem, src_phi, rcv_elem, rcv_phi, precision="fp64",
-                    device=0):
+                    device=0, ref_invmass=None):
+        """ref_invmass: the reference inverse mass [Np][Np] of a
+        non-orthonormal basis (None for Dubiner)."""
+        ref_invmass = None if ref_invmass is None else _f64(ref_invmass)
         row_ptr, col = _i32(row_ptr), _i32(col)
         blocks, minv = _f64(blocks), _f64(minv)
         src_elem, src_phi = _i32(np.atleast_1d(src_elem)), _f64(np.atleast_2d(src_phi))
@@ -223,7 +231,8 @@ class Simulation:
         Np = blocks.shape[1] // 2
         p = TspBlockProblem(ne, Np, col.shape[0], _i(row_ptr), _i(col), _d(blocks), _d(minv), TSP_PREC[precision],
                             src_elem.shape[0], _i(src_elem), _d(src_phi), rcv_elem.shape[0],
-                            _i(rcv_elem) if len(rcv_elem) else None, _d(rcv_phi) if len(rcv_elem) else None, device)
+                            _i(rcv_elem) if len(rcv_elem) else None, _d(rcv_phi) if len(rcv_elem) else None, device,
+                            _d(ref_invmass))
         h = C.c_void_p()
         _check(lib().tsp_create_from_blocks(C.byref(p), C.byref(h)))
         return cls(h)
@@ -290,6 +299,18 @@ class Simulation:
         v = C.c_int32()
         _check(lib().tsp_get_kernel_variant(self._h, C.byref(v)), self._h)
         return v.value
+
+    @property
+    def basis(self) -> str:
+        b = C.c_int32()
+        _check(lib().tsp_get_ref_invmass(self._h, C.byref(b), None), self._h)
+        return "dubiner" if b.value == 0 else "ba"
+
+    def ref_invmass(self):
+        """M_ref^-1 of the handle's basis, [Np][Np] (identity for Dubiner)."""
+        out = np.zeros((self.Np, self.Np))
+        _check(lib().tsp_get_ref_invmass(self._h, None, _d(out)), self._h)
+        return out
 
     # ---- outputs ----
     def u(self, shot: int = 0):

@@ -33,6 +33,16 @@ struct tsp_handle {
   long long nnzb = 0;
   int prec = TSP_PREC_FP64, op_kind = TSP_OP_EXPLICIT;
   int bpitch = 0;  // column pitch of stored blocks: 2Np (one shot) or 2Np rounded up to 4 (batched)
+  // Non-orthonormal basis (BoundaryAdapted): M_ref = L L^T (Cholesky). The
+  // device works in the orthonormalised coordinates w = L^T u of every
+  // element and component: blocks L^-1 B L^-T, source and receiver values
+  // L^-1 phi, per-element mass rho detJ I as for Dubiner, so every kernel
+  // (the energy monitor included) runs unchanged. Host vectors stay in the
+  // reference's coefficients u; the maps are applied at the boundary.
+  // Empty for the orthonormal Dubiner basis. [Np][Np] row-major.
+  int basis = tsp::kDubiner;
+  std::vector<double> minv_ref, lref, lref_inv;
+  double* d_lref_inv = nullptr;
   // operator
   int* d_row_ptr = nullptr;
   int* d_col = nullptr;
@@ -138,6 +148,29 @@ int upload(tsp_handle* h, T** d, const T* src, size_t n) {
   return TSP_OK;
 }
 
+// v <- A v (trans = false) or A^T v (trans = true) for nvec consecutive
+// Np-vectors, A [Np][Np] row-major.
+void map_vectors(const std::vector<double>& A, bool trans, int Np, double* v, long long nvec) {
+  double t[tsp::kFoldMaxNp];
+  for (long long r = 0; r < nvec; ++r) {
+    double* x = v + size_t(r) * Np;
+    for (int i = 0; i < Np; ++i) {
+      double a = 0.0;
+      for (int j = 0; j < Np; ++j) a += (trans ? A[size_t(j) * Np + i] : A[size_t(i) * Np + j]) * x[j];
+      t[i] = a;
+    }
+    std::memcpy(x, t, Np * sizeof(double));
+  }
+}
+// Reference coefficients u -> device coordinates w = L^T u, and back
+// u = L^-T w, for nvec Np-vectors in place. No-ops for Dubiner.
+void to_dev_coords(const tsp_handle* h, double* v, long long nvec) {
+  if (!h->lref.empty()) map_vectors(h->lref, true, h->Np, v, nvec);
+}
+void to_ref_coords(const tsp_handle* h, double* v, long long nvec) {
+  if (!h->lref_inv.empty()) map_vectors(h->lref_inv, true, h->Np, v, nvec);
+}
+
 void clear_graphs(tsp_handle* h) {
   for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
   h->graphs.clear();
@@ -154,7 +187,9 @@ int build_receiver_csr(tsp_handle* h) {
   int rc;
   if ((rc = upload(h, &h->d_rcv_ptr, ptr.data(), ptr.size()))) return rc;
   if ((rc = upload(h, &h->d_rcv_id, ids.data(), ids.size()))) return rc;
-  if ((rc = upload(h, &h->d_rcv_phi, h->rcv_phi.data(), h->rcv_phi.size()))) return rc;
+  std::vector<double> rphi(h->rcv_phi);
+  if (!h->lref_inv.empty()) map_vectors(h->lref_inv, false, h->Np, rphi.data(), h->nrcv);
+  if ((rc = upload(h, &h->d_rcv_phi, rphi.data(), rphi.size()))) return rc;
   return TSP_OK;
 }
 
@@ -297,6 +332,28 @@ int autotune(tsp_handle* h) {
 }
 
 // Common tail of both constructors: state, step counter, sources, receivers.
+// Sets up a non-orthonormal basis from its reference mass M_ref.
+int set_basis_mass(tsp_handle* h, int basis, const std::vector<double>& mass, const std::vector<double>& minv) {
+  h->basis = basis;
+  h->minv_ref = minv;
+  if (!tsp::cholesky(h->Np, mass, &h->lref, &h->lref_inv))
+    return fail(h, TSP_ERR_ARG, "reference mass is not symmetric positive definite");
+  return upload(h, &h->d_lref_inv, h->lref_inv.data(), h->lref_inv.size());
+}
+
+// Turns FP64 blocks B on the device (column-major, pitch pin; overwritten)
+// into L^-1 B L^-T in the handle's storage type at h->d_blocks.
+int fold_blocks(tsp_handle* h, double* d_in, int pin) {
+  tsp::k_fold_basis<<<unsigned(h->nnzb), 256, 0, h->stream>>>(d_in, pin, h->Np, h->d_lref_inv, 0, TSP_PREC_FP64, pin,
+                                                             d_in, nullptr);
+  tsp::k_fold_basis<<<unsigned(h->nnzb), 256, 0, h->stream>>>(d_in, pin, h->Np, h->d_lref_inv, 1, h->prec, h->bpitch,
+                                                             h->d_blocks, h->d_bscale);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+  if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("basis fold: ") + cudaGetErrorString(ce));
+  return TSP_OK;
+}
+
 int finish_create(tsp_handle* h) {
   int rc;
   const size_t nstate = size_t(h->ne) * h->S * h->R;
@@ -326,7 +383,13 @@ int finish_create(tsp_handle* h) {
   TSP_CUDA(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
   if ((rc = dalloc(h, &h->d_acc, 3))) return rc;
   if ((rc = upload(h, &h->d_src_elem, h->src_elem.data(), h->src_elem.size()))) return rc;
-  if ((rc = upload(h, &h->d_src_phi, h->src_phi.data(), h->src_phi.size()))) return rc;
+  {
+    // Device coordinates: the force vector L^-1 f and the receiver functional
+    // u -> phi^T u = (L^-1 phi)^T w both take L^-1 phi.
+    std::vector<double> sphi(h->src_phi);
+    if (!h->lref_inv.empty()) map_vectors(h->lref_inv, false, h->Np, sphi.data(), h->S);
+    if ((rc = upload(h, &h->d_src_phi, sphi.data(), sphi.size()))) return rc;
+  }
   if ((rc = build_receiver_csr(h))) return rc;
   long long cap = 4096;
   if (h->nrcv > 0) {
@@ -604,19 +667,24 @@ int launch_step_params(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st)
 }
 
 // Reference layout u[c*ne*Np + e*Np + i] <-> device layout [(e*S+s)*R + c*Np + i].
+// The device holds w = L^T u (u itself for Dubiner).
 void ref_to_dev(const tsp_handle* h, int shot, const double* src, double* dst_all) {
   const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
-  for (int e = 0; e < ne; ++e)
+  for (int e = 0; e < ne; ++e) {
+    double* d = dst_all + (size_t(e) * S + shot) * R;
     for (int c = 0; c < 2; ++c)
-      std::memcpy(dst_all + (size_t(e) * S + shot) * R + size_t(c) * Np, src + size_t(c) * ne * Np + size_t(e) * Np,
-                  Np * sizeof(double));
+      std::memcpy(d + size_t(c) * Np, src + size_t(c) * ne * Np + size_t(e) * Np, Np * sizeof(double));
+    to_dev_coords(h, d, 2);
+  }
 }
 void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* dst) {
   const int ne = h->ne, Np = h->Np, R = h->R, S = h->S;
-  for (int e = 0; e < ne; ++e)
-    for (int c = 0; c < 2; ++c)
-      std::memcpy(dst + size_t(c) * ne * Np + size_t(e) * Np, src_all + (size_t(e) * S + shot) * R + size_t(c) * Np,
-                  Np * sizeof(double));
+  double t[2 * tsp::kFoldMaxNp];
+  for (int e = 0; e < ne; ++e) {
+    std::memcpy(t, src_all + (size_t(e) * S + shot) * R, R * sizeof(double));
+    to_ref_coords(h, t, 2);
+    for (int c = 0; c < 2; ++c) std::memcpy(dst + size_t(c) * ne * Np + size_t(e) * Np, t + c * Np, Np * sizeof(double));
+  }
 }
 
 
@@ -638,6 +706,7 @@ int get_shot(tsp_handle* h, const double* dsrc, int shot, double* out) {
                                 size_t(h->S) * R * sizeof(double), size_t(R) * sizeof(double), ne,
                                 cudaMemcpyDeviceToHost, h->stream));
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  to_ref_coords(h, slice.data(), 2ll * ne);
   for (int e = 0; e < ne; ++e)
     for (int c = 0; c < 2; ++c)
       std::memcpy(out + size_t(c) * ne * h->Np + size_t(e) * h->Np, &slice[size_t(e) * R + size_t(c) * h->Np],
@@ -652,6 +721,7 @@ int put_shot(tsp_handle* h, double* ddst, int shot, const double* in) {
       for (int c = 0; c < 2; ++c)
         std::memcpy(&slice[size_t(e) * R + size_t(c) * h->Np], in + size_t(c) * ne * h->Np + size_t(e) * h->Np,
                     h->Np * sizeof(double));
+  to_dev_coords(h, slice.data(), 2ll * ne);
   TSP_CUDA(h, cudaMemcpy2DAsync(ddst + size_t(shot) * R, size_t(h->S) * R * sizeof(double), slice.data(),
                                 size_t(R) * sizeof(double), size_t(R) * sizeof(double), ne, cudaMemcpyHostToDevice,
                                 h->stream));
@@ -712,6 +782,10 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
     return fail(nullptr, TSP_ERR_ARG, "bad operator kind");
   if (P->op_kind == TSP_OP_MATRIX_FREE && (P->precision != TSP_PREC_FP64 || P->nshots != 1))
     return fail(nullptr, TSP_ERR_UNSUPPORTED, "the matrix-free operator runs FP64 with one shot per handle");
+  if (P->basis != TSP_BASIS_DUBINER && P->basis != TSP_BASIS_BOUNDARY_ADAPTED)
+    return fail(nullptr, TSP_ERR_ARG, "bad basis");
+  if (P->basis != TSP_BASIS_DUBINER && P->op_kind == TSP_OP_MATRIX_FREE)
+    return fail(nullptr, TSP_ERR_UNSUPPORTED, "the matrix-free operator is built for the orthonormal Dubiner basis");
   for (int32_t i = 0; i < 3 * P->ne; ++i)
     if (P->tri[i] < 0 || P->tri[i] >= P->nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
   for (int32_t e = 0; e < P->ne; ++e)
@@ -729,6 +803,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   h->nrcv = P->nrcv;
   h->prec = P->precision;
   h->op_kind = P->op_kind;
+  h->basis = P->basis;
 
   // ---- host setup: geometry, neighbours, pattern, tables ----
   tsp::Geometry g = tsp::make_geometry(P->ne, P->xy, P->tri);
@@ -749,14 +824,15 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   std::vector<int8_t> bface;
   tsp::bsr_pattern(P->ne, neigh.data(), &row_ptr, &col, &bface);
   h->nnzb = (long long)col.size();
-  tsp::RefTables T = tsp::make_tables(P->N);
+  tsp::RefTables T = tsp::make_tables(P->N, P->basis);
+  if (P->basis != TSP_BASIS_DUBINER && (rc = set_basis_mass(h, P->basis, T.M, T.Minv))) return create_error_from(h, rc);
 
   // ---- sources and receivers ----
   h->src_elem.resize(h->S);
   h->src_phi.resize(size_t(h->S) * h->Np);
   for (int s = 0; s < h->S; ++s) {
     const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->src_xy[2 * s], P->src_xy[2 * s + 1],
-                                    &h->src_phi[size_t(s) * h->Np]);
+                                    &h->src_phi[size_t(s) * h->Np], P->basis);
     if (e < 0) {
       fail(h, TSP_ERR_NOT_FOUND, "source point " + std::to_string(s) + " not found in the mesh");
       return create_error_from(h, TSP_ERR_NOT_FOUND);
@@ -767,7 +843,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   h->rcv_phi.resize(size_t(h->nrcv) * h->Np);
   for (int r = 0; r < h->nrcv; ++r) {
     const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->rcv_xy[2 * r], P->rcv_xy[2 * r + 1],
-                                    &h->rcv_phi[size_t(r) * h->Np]);
+                                    &h->rcv_phi[size_t(r) * h->Np], P->basis);
     if (e < 0) {
       fail(h, TSP_ERR_NOT_FOUND, "receiver point " + std::to_string(r) + " not found in the mesh");
       return create_error_from(h, TSP_ERR_NOT_FOUND);
@@ -877,6 +953,17 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   ap.pitch = h->bpitch;
   ap.out = h->d_blocks;
   ap.scale = h->d_bscale;
+  // Non-orthonormal basis: assemble B in FP64 (in place for FP64 storage,
+  // else in a temporary at pitch 2Np), then map it to L^-1 B L^-T.
+  double* d_tmp = nullptr;
+  if (!h->lref.empty()) {
+    ap.prec = TSP_PREC_FP64;
+    if (h->prec != TSP_PREC_FP64) {
+      if ((rc = dalloc(h, &d_tmp, size_t(h->nnzb) * h->R * h->R))) return create_error_from(h, rc);
+      ap.out = d_tmp;
+      ap.pitch = h->R;
+    }
+  }
   // Large meshes exceed the 2^31-1 grid limit only beyond 2 G blocks.
   tsp::k_assemble<<<unsigned(h->nnzb), 256, 0, h->stream>>>(ap);
   {
@@ -886,6 +973,11 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
       fail(h, TSP_ERR_CUDA, std::string("assembly kernel: ") + cudaGetErrorString(ce));
       return create_error_from(h, TSP_ERR_CUDA);
     }
+  }
+  if (!h->lref.empty()) {
+    rc = fold_blocks(h, d_tmp ? d_tmp : reinterpret_cast<double*>(h->d_blocks), ap.pitch);
+    if (d_tmp) dfree(h, d_tmp);
+    if (rc) return create_error_from(h, rc);
   }
   for (void* q : {(void*)d_neigh, (void*)d_nedge, (void*)d_bface, (void*)d_invJ, (void*)d_detJ, (void*)d_elen,
                   (void*)d_enrm, (void*)d_lam, (void*)d_mu, (void*)d_K, (void*)d_Ws, (void*)d_Wx, (void*)d_Ds,
@@ -919,6 +1011,12 @@ int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
     if (P->src_elem[s] < 0 || P->src_elem[s] >= P->ne) return fail(nullptr, TSP_ERR_ARG, "source element out of range");
   for (int r = 0; r < P->nrcv; ++r)
     if (P->rcv_elem[r] < 0 || P->rcv_elem[r] >= P->ne) return fail(nullptr, TSP_ERR_ARG, "receiver element out of range");
+  std::vector<double> mref, mi;
+  if (P->ref_invmass) {
+    mi.assign(P->ref_invmass, P->ref_invmass + size_t(P->Np) * P->Np);
+    if (!tsp::spd_inverse(P->Np, mi, &mref))
+      return fail(nullptr, TSP_ERR_ARG, "ref_invmass is not symmetric positive definite");
+  }
 
   tsp_handle* h = nullptr;
   int rc = make_handle(P->device, &h);
@@ -931,6 +1029,7 @@ int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
   h->nrcv = P->nrcv;
   h->prec = P->precision;
   h->nnzb = P->nnzb;
+  if (P->ref_invmass && (rc = set_basis_mass(h, TSP_BASIS_BOUNDARY_ADAPTED, mref, mi))) return create_error_from(h, rc);
   h->src_elem.assign(P->src_elem, P->src_elem + h->S);
   h->src_phi.assign(P->src_phi, P->src_phi + size_t(h->S) * h->Np);
   h->rcv_elem.assign(P->rcv_elem, P->rcv_elem + h->nrcv);
@@ -943,6 +1042,28 @@ int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
   const size_t RR = size_t(R) * R;
   h->bpitch = block_pitch(R, h->S);
   const int BP = h->bpitch;
+  if (!h->lref.empty()) {
+    // FP64 column-major copy on the device, mapped to L^-1 B L^-T there.
+    std::vector<double> cm(size_t(P->nnzb) * RR);
+    for (int b = 0; b < P->nnzb; ++b)
+      for (int r = 0; r < R; ++r)
+        for (int c = 0; c < R; ++c) cm[size_t(b) * RR + size_t(c) * R + r] = P->blocks[size_t(b) * RR + size_t(r) * R + c];
+    double* d_tmp = nullptr;
+    const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
+    if ((rc = upload(h, &d_tmp, cm.data(), cm.size()))) return create_error_from(h, rc);
+    std::vector<double>().swap(cm);
+    unsigned char* dblk = nullptr;
+    if ((rc = dalloc(h, &dblk, size_t(P->nnzb) * R * BP * esz))) return create_error_from(h, rc);
+    h->d_blocks = dblk;
+    TSP_CUDA(h, cudaMemsetAsync(h->d_blocks, 0, size_t(P->nnzb) * R * BP * esz, h->stream));
+    if (h->prec == TSP_PREC_BF16 && (rc = dalloc(h, &h->d_bscale, size_t(P->nnzb)))) return create_error_from(h, rc);
+    rc = fold_blocks(h, d_tmp, R);
+    dfree(h, d_tmp);
+    if (rc) return create_error_from(h, rc);
+    if ((rc = finish_create(h))) return create_error_from(h, rc);
+    *out = h;
+    return TSP_OK;
+  }
   const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
   std::vector<unsigned char> host(size_t(P->nnzb) * R * BP * esz, 0);
   std::vector<float> scales(h->prec == TSP_PREC_BF16 ? size_t(P->nnzb) : 0);
@@ -1205,7 +1326,8 @@ int tsp_get_u_all(tsp_handle* h, double* out) {
   if ((rc = dalloc(h, &tmp, nref * chunk))) return rc;
   for (int s0 = 0; s0 < h->S && rc == TSP_OK; s0 += chunk) {
     const int ns = std::min(chunk, h->S - s0);
-    tsp::k_state_to_ref<<<1184, 256, 0, h->stream>>>(h->d_U[h->cur], h->ne, h->S, h->Np, s0, ns, tmp);
+    tsp::k_state_to_ref<<<1184, 256, 0, h->stream>>>(h->d_U[h->cur], h->ne, h->S, h->Np, s0, ns, tmp,
+                                                     h->d_lref_inv);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(out + size_t(s0) * nref, tmp, nref * ns * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
@@ -1353,11 +1475,13 @@ int tsp_apply(tsp_handle* h, const double* x, double* y) {
     for (int c = 0; c < 2; ++c)
       std::memcpy(&v[size_t(e) * h->R + size_t(c) * h->Np], x + size_t(c) * h->ne * h->Np + size_t(e) * h->Np,
                   h->Np * sizeof(double));
+  to_dev_coords(h, v.data(), 2ll * h->ne);  // B x = L (L^-1 B L^-T) (L^T x)
   TSP_CUDA(h, cudaMemcpy(dx, v.data(), n1 * sizeof(double), cudaMemcpyHostToDevice));
   if ((rc = launch_step(h, tsp::kModeApply, dx, nullptr, dy, 0, 1.0, h->stream))) return rc;
   TSP_CUDA(h, cudaGetLastError());
   TSP_CUDA(h, cudaMemcpyAsync(v.data(), dy, n1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!h->lref.empty()) map_vectors(h->lref, false, h->Np, v.data(), 2ll * h->ne);
   for (int e = 0; e < h->ne; ++e)
     for (int c = 0; c < 2; ++c)
       std::memcpy(y + size_t(c) * h->ne * h->Np + size_t(e) * h->Np, &v[size_t(e) * h->R + size_t(c) * h->Np],
@@ -1432,6 +1556,22 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
           else v = double(__bfloat162float(reinterpret_cast<__nv_bfloat16*>(raw.data())[i])) * sc[b];
           blocks[size_t(b) * RR + size_t(r) * h->R + c] = v;
         }
+    if (!h->lref.empty()) {
+      // Stored: L^-1 B L^-T; exported: B = L (L^-1 B L^-T) L^T, applied to
+      // the Np-segments of every row (right factor) and column (left factor).
+      const int Np = h->Np, R = h->R;
+      std::vector<double> col(Np);
+      for (long long b = 0; b < h->nnzb; ++b) {
+        double* blk = blocks + size_t(b) * RR;
+        for (int r = 0; r < R; ++r) map_vectors(h->lref, false, Np, blk + size_t(r) * R, 2);
+        for (int c = 0; c < R; ++c)
+          for (int comp = 0; comp < 2; ++comp) {
+            for (int j = 0; j < Np; ++j) col[j] = blk[size_t(comp * Np + j) * R + c];
+            map_vectors(h->lref, false, Np, col.data(), 1);
+            for (int j = 0; j < Np; ++j) blk[size_t(comp * Np + j) * R + c] = col[j];
+          }
+      }
+    }
   }
   return TSP_OK;
 }
@@ -1471,13 +1611,32 @@ int tsp_quadrature_points(int32_t N, int32_t nverts, const double* xy, int32_t n
   return TSP_OK;
 }
 
-int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
-                double* out) {
+int tsp_project_basis(int32_t N, int32_t basis, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri,
+                      const double* fvals, double* out) {
   if (N < 1 || N > tsp::kMaxN || nverts <= 0 || ne <= 0 || !xy || !tri || !fvals || !out)
     return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_project");
+  if (basis != TSP_BASIS_DUBINER && basis != TSP_BASIS_BOUNDARY_ADAPTED) return fail(nullptr, TSP_ERR_ARG, "bad basis");
   for (int32_t i = 0; i < 3 * ne; ++i)
     if (tri[i] < 0 || tri[i] >= nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
-  tsp::project(N, ne, xy, tri, fvals, out);
+  tsp::project(N, ne, xy, tri, fvals, out, basis);
+  return TSP_OK;
+}
+
+int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
+                double* out) {
+  return tsp_project_basis(N, TSP_BASIS_DUBINER, nverts, xy, ne, tri, fvals, out);
+}
+
+int tsp_get_ref_invmass(const tsp_handle* h, int32_t* basis, double* out) {
+  if (!h) return TSP_ERR_ARG;
+  if (basis) *basis = h->basis;
+  if (out) {
+    const size_t n = size_t(h->Np) * h->Np;
+    if (h->minv_ref.empty())
+      for (size_t i = 0; i < n; ++i) out[i] = (i % (size_t(h->Np) + 1) == 0) ? 1.0 : 0.0;
+    else
+      std::copy(h->minv_ref.begin(), h->minv_ref.end(), out);
+  }
   return TSP_OK;
 }
 
@@ -1640,6 +1799,8 @@ int tsp_batch_create(const tsp_problem* meshes, int32_t nmesh, tsp_batch** out) 
     if (P.nshots != 1 || !P.src_xy) return bfail(nullptr, TSP_ERR_ARG, "each mesh of a batch has exactly one source");
     if (P.precision != prec || P.op_kind != op || P.device != dev)
       return bfail(nullptr, TSP_ERR_ARG, "all meshes of a batch share precision, operator kind and device");
+    if (P.basis != TSP_BASIS_DUBINER)
+      return bfail(nullptr, TSP_ERR_UNSUPPORTED, "multi-mesh batches are built for the Dubiner basis");
     if (P.N < 1 || P.N > tsp::kMaxN || P.ne <= 0 || P.nverts <= 0 || !P.xy || !P.tri || !P.lambda || !P.mu || !P.rho)
       return bfail(nullptr, TSP_ERR_ARG, "mesh " + std::to_string(m) + ": bad problem");
     if (P.nrcv < 0 || (P.nrcv > 0 && !P.rcv_xy)) return bfail(nullptr, TSP_ERR_ARG, "bad receivers");

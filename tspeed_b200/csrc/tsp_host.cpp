@@ -37,6 +37,7 @@ void gauleg(int n, double a, double b, double* x, double* w) {
 }
 
 double jacobi(int n, int alpha, int beta, double z) {
+  if (n < 0) return 0.0;
   if (n == 0) return 1.0;
   const double p1_0 = 0.5 * (alpha - beta + (alpha + beta + 2.0) * z);
   if (n == 1) return p1_0;
@@ -98,6 +99,131 @@ void dubiner_grad(int N, double csi, double eta, double* gc, double* ge) {
     }
 }
 
+// (1-eta)^(i-1) P^{1,1}_{i-1}(2 csi/(1-eta) - 1), a polynomial of degree i-1
+// in (csi, eta); its value at the collapsed vertex (0, 1) is 1 for i = 1 and
+// 0 above.
+static double ba_radial(int i, double csi, double om) {
+  if (om == 0.0) return i == 1 ? 1.0 : 0.0;
+  return std::pow(om, i - 1) * jacobi(i - 1, 1, 1, 2 * csi / om - 1);
+}
+
+void ba_phi(int N, double csi, double eta, double* phi) {
+  const double l0 = 1 - csi - eta, om = 1 - eta, yy = 2 * eta - 1;
+  int s = 0;
+  phi[s++] = l0;
+  phi[s++] = csi;
+  phi[s++] = eta;
+  for (int i = 1; i < N; ++i) phi[s++] = l0 * csi * ba_radial(i, csi, om);
+  for (int j = 1; j < N; ++j) phi[s++] = l0 * eta * jacobi(j - 1, 1, 1, yy);
+  for (int j = 1; j < N; ++j) phi[s++] = csi * eta * jacobi(j - 1, 1, 1, yy);
+  for (int j = 1; j < N; ++j)
+    for (int i = 1; i + j < N; ++i) phi[s++] = l0 * csi * eta * ba_radial(i, csi, om) * jacobi(j - 1, 2 * i + 1, 1, yy);
+}
+
+void ba_grad(int N, double csi, double eta, double* gc, double* ge) {
+  const double l0 = 1 - csi - eta, om = 1 - eta, yy = 2 * eta - 1, xx = 2 * csi / om - 1;
+  int s = 0;
+  gc[s] = -1; ge[s++] = -1;
+  gc[s] = 1;  ge[s++] = 0;
+  gc[s] = 0;  ge[s++] = 1;
+  // Family A, l0 csi (1-eta)^(i-1) P^{1,1}_{i-1}(xx), using
+  // d/dz P^{a,b}_n = (n + a + b + 1)/2 P^{a+1,b+1}_{n-1} and
+  // dxx/dcsi = 2/(1-eta), dxx/deta = 2 csi/(1-eta)^2.
+  for (int i = 1; i < N; ++i, ++s) {
+    const double pa = jacobi(i - 1, 1, 1, xx), dp = jacobi(i - 2, 2, 2, xx);
+    gc[s] = (1 - 2 * csi - eta) * std::pow(om, i - 1) * pa + l0 * csi * std::pow(om, i - 2) * dp * (i + 2);
+    ge[s] = -std::pow(om, i - 2) * csi * (i + csi - i * csi - i * eta) * pa +
+            csi * csi * l0 * std::pow(om, i - 3) * (i + 2) * dp;
+  }
+  // Family B, l0 eta P^{1,1}_{j-1}(2 eta - 1).
+  for (int j = 1; j < N; ++j, ++s) {
+    const double pj = jacobi(j - 1, 1, 1, yy);
+    gc[s] = -eta * pj;
+    ge[s] = (1 - csi - 2 * eta) * pj + l0 * eta * jacobi(j - 2, 2, 2, yy) * (j + 2);
+  }
+  // Family C, csi eta P^{1,1}_{j-1}(2 eta - 1).
+  for (int j = 1; j < N; ++j, ++s) {
+    const double pj = jacobi(j - 1, 1, 1, yy);
+    gc[s] = eta * pj;
+    ge[s] = csi * pj + eta * csi * (j + 2) * jacobi(j - 2, 2, 2, yy);
+  }
+  // Interior, l0 csi eta (1-eta)^(i-1) P^{1,1}_{i-1}(xx) P^{2i+1,1}_{j-1}(2 eta - 1).
+  for (int j = 1; j < N; ++j)
+    for (int i = 1; i + j < N; ++i, ++s) {
+      const double pa = jacobi(i - 1, 1, 1, xx), dpa = jacobi(i - 2, 2, 2, xx);
+      const double pb = jacobi(j - 1, 2 * i + 1, 1, yy), dpb = jacobi(j - 2, 2 * i + 2, 2, yy);
+      gc[s] = eta * std::pow(om, i - 2) * pb * ((1 - 2 * csi - eta) * om * pa + l0 * csi * (i + 2) * dpa);
+      ge[s] = csi * std::pow(om, i - 3) *
+              ((om * om * (1 - csi - 2 * eta) - om * eta * l0 * (i - 1)) * pa * pb + csi * l0 * eta * (i + 2) * dpa * pb +
+               l0 * eta * om * om * (j + 2 * i + 2) * pa * dpb);
+    }
+}
+
+void basis_phi(int basis, int N, double csi, double eta, double* phi) {
+  if (basis == kBoundaryAdapted) ba_phi(N, csi, eta, phi);
+  else dubiner_phi(N, csi, eta, phi);
+}
+
+void basis_grad(int basis, int N, double csi, double eta, double* gc, double* ge) {
+  if (basis == kBoundaryAdapted) ba_grad(N, csi, eta, gc, ge);
+  else dubiner_grad(N, csi, eta, gc, ge);
+}
+
+bool spd_inverse(int n, const std::vector<double>& A, std::vector<double>* Ainv) {
+  std::vector<double> L(size_t(n) * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = A[size_t(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= L[size_t(j) * n + k] * L[size_t(j) * n + k];
+    if (!(d > 0)) return false;
+    L[size_t(j) * n + j] = std::sqrt(d);
+    for (int i = j + 1; i < n; ++i) {
+      double v = A[size_t(i) * n + j];
+      for (int k = 0; k < j; ++k) v -= L[size_t(i) * n + k] * L[size_t(j) * n + k];
+      L[size_t(i) * n + j] = v / L[size_t(j) * n + j];
+    }
+  }
+  // Columns of A^-1: solve L L^T x = e_c.
+  Ainv->assign(size_t(n) * n, 0.0);
+  std::vector<double> y(n);
+  for (int c = 0; c < n; ++c) {
+    for (int i = 0; i < n; ++i) {
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) v -= L[size_t(i) * n + k] * y[k];
+      y[i] = v / L[size_t(i) * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double v = y[i];
+      for (int k = i + 1; k < n; ++k) v -= L[size_t(k) * n + i] * (*Ainv)[size_t(k) * n + c];
+      (*Ainv)[size_t(i) * n + c] = v / L[size_t(i) * n + i];
+    }
+  }
+  return true;
+}
+
+bool cholesky(int n, const std::vector<double>& A, std::vector<double>* L, std::vector<double>* Linv) {
+  L->assign(size_t(n) * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = A[size_t(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= (*L)[size_t(j) * n + k] * (*L)[size_t(j) * n + k];
+    if (!(d > 0)) return false;
+    (*L)[size_t(j) * n + j] = std::sqrt(d);
+    for (int i = j + 1; i < n; ++i) {
+      double v = A[size_t(i) * n + j];
+      for (int k = 0; k < j; ++k) v -= (*L)[size_t(i) * n + k] * (*L)[size_t(j) * n + k];
+      (*L)[size_t(i) * n + j] = v / (*L)[size_t(j) * n + j];
+    }
+  }
+  // L^-1 by forward substitution, column by column (lower triangular).
+  Linv->assign(size_t(n) * n, 0.0);
+  for (int c = 0; c < n; ++c)
+    for (int i = c; i < n; ++i) {
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) v -= (*L)[size_t(i) * n + k] * (*Linv)[size_t(k) * n + c];
+      (*Linv)[size_t(i) * n + c] = v / (*L)[size_t(i) * n + i];
+    }
+  return true;
+}
+
 static void edge_node(int l, double x, double* c, double* e) {
   // QuadratureRule_imp.hpp:66-91.
   if (l == 2) { *c = x; *e = 0.0; }
@@ -105,9 +231,10 @@ static void edge_node(int l, double x, double* c, double* e) {
   else { *c = 0.0; *e = 1.0 - x; }
 }
 
-RefTables make_tables(int N) {
+RefTables make_tables(int N, int basis) {
   RefTables T;
   T.N = N;
+  T.basis = basis;
   T.Np = np_of(N);
   T.Q = N + 1;
   const int Np = T.Np, Q = T.Q;
@@ -123,7 +250,7 @@ RefTables make_tables(int N) {
     for (int j = 0; j < Q; ++j) {
       const double wq = (1 - x[i]) * w[i] * w[j] / 8.;
       const double c = (1 + x[i]) / 2., e = (1 - x[i]) * (1 + x[j]) / 4.;
-      dubiner_grad(N, c, e, gc.data(), ge.data());
+      basis_grad(basis, N, c, e, gc.data(), ge.data());
       const double* g[2] = {gc.data(), ge.data()};
       for (int a = 0; a < 2; ++a)
         for (int b = 0; b < 2; ++b)
@@ -137,8 +264,9 @@ RefTables make_tables(int N) {
     for (int k = 0; k < Q; ++k) {
       double c, e;
       edge_node(l, x1[k], &c, &e);
-      dubiner_phi(N, c, e, &T.Be[(size_t(l) * Q + k) * Np]);
-      dubiner_grad(N, c, e, &T.Ge[((size_t(l) * 2 + 0) * Q + k) * Np], &T.Ge[((size_t(l) * 2 + 1) * Q + k) * Np]);
+      basis_phi(basis, N, c, e, &T.Be[(size_t(l) * Q + k) * Np]);
+      basis_grad(basis, N, c, e, &T.Ge[((size_t(l) * 2 + 0) * Q + k) * Np],
+                 &T.Ge[((size_t(l) * 2 + 1) * Q + k) * Np]);
     }
   auto B = [&](int l, int k, int i) { return T.Be[(size_t(l) * Q + k) * Np + i]; };
   auto G = [&](int l, int a, int k, int i) { return T.Ge[((size_t(l) * 2 + a) * Q + k) * Np + i]; };
@@ -160,6 +288,25 @@ RefTables make_tables(int N) {
           }
         }
     }
+  // Reference mass on the collapsed Gauss<N+1> rule: the integrand has degree
+  // 2N, which the rule integrates exactly (the reference uses Dunavant<2N>
+  // for BoundaryAdapted, equal up to rounding).
+  T.Minv.assign(P2, 0.0);
+  if (basis == kDubiner) {
+    for (int i = 0; i < Np; ++i) T.Minv[size_t(i) * Np + i] = 1.0;
+    T.M = T.Minv;
+  } else {
+    std::vector<double> M(P2, 0.0), ph(Np);
+    for (int i = 0; i < Q; ++i)
+      for (int j = 0; j < Q; ++j) {
+        const double wq = (1 - x[i]) * w[i] * w[j] / 8.;
+        basis_phi(basis, N, (1 + x[i]) / 2., (1 - x[i]) * (1 + x[j]) / 4., ph.data());
+        for (int r = 0; r < Np; ++r)
+          for (int c = 0; c < Np; ++c) M[size_t(r) * Np + c] += wq * ph[r] * ph[c];
+      }
+    spd_inverse(Np, M, &T.Minv);
+    T.M = M;
+  }
   return T;
 }
 
@@ -252,7 +399,7 @@ void bsr_pattern(int32_t ne, const int32_t* neigh, std::vector<int32_t>* row_ptr
 }
 
 int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, double px,
-                     double py, double* phi) {
+                     double py, double* phi, int basis) {
   for (int32_t e = 0; e < ne; ++e) {
     const double* p0 = xy + 2 * size_t(tri[3 * size_t(e)]);
     const double* p1 = xy + 2 * size_t(tri[3 * size_t(e) + 1]);
@@ -271,7 +418,7 @@ int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, co
       const double dx = px - p0[0], dy = py - p0[1];
       const double r0 = iJ[0] * dx + iJ[2] * dy;
       const double r1 = iJ[1] * dx + iJ[3] * dy;
-      dubiner_phi(N, r0, r1, phi);
+      basis_phi(basis, N, r0, r1, phi);
       return e;
     }
   }
@@ -387,13 +534,14 @@ void quadrature_points(int N, int32_t ne, const double* xy, const int32_t* tri, 
   }
 }
 
-void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out) {
+void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out, int basis) {
   std::vector<double> c, e, w;
   volume_rule(N, &c, &e, &w);
   const size_t nq = c.size();
   const int Np = np_of(N);
   std::vector<double> B(nq * Np);  // basis at the volume points, [q][i]
-  for (size_t q = 0; q < nq; ++q) dubiner_phi(N, c[q], e[q], &B[q * Np]);
+  for (size_t q = 0; q < nq; ++q) basis_phi(basis, N, c[q], e[q], &B[q * Np]);
+  const RefTables T = make_tables(N, basis);
   const Geometry g = make_geometry(ne, xy, tri);
   std::vector<double> rhs(2 * size_t(Np));
   for (int32_t el = 0; el < ne; ++el) {
@@ -406,11 +554,16 @@ void project(int N, int32_t ne, const double* xy, const int32_t* tri, const doub
         rhs[Np + i] += F[1] * dx * B[q * Np + i];
       }
     }
-    // Orthonormal basis: the reference mass is the identity (FESpace_imp.hpp:51-54),
-    // uh = 1/detJ * rhs (FESpace_imp.hpp:152-153).
+    // uh = 1/detJ * M_ref^-1 * rhs (FESpace_imp.hpp:152-153); M_ref^-1 is the
+    // identity for the orthonormal Dubiner basis (FESpace_imp.hpp:51-54).
     for (int i = 0; i < Np; ++i) {
-      out[size_t(el) * Np + i] = 1. / g.detJ[el] * rhs[i];
-      out[size_t(ne) * Np + size_t(el) * Np + i] = 1. / g.detJ[el] * rhs[Np + i];
+      double a0 = 0.0, a1 = 0.0;
+      for (int j = 0; j < Np; ++j) {
+        a0 += T.Minv[size_t(i) * Np + j] * rhs[j];
+        a1 += T.Minv[size_t(i) * Np + j] * rhs[Np + j];
+      }
+      out[size_t(el) * Np + i] = 1. / g.detJ[el] * a0;
+      out[size_t(ne) * Np + size_t(el) * Np + i] = 1. / g.detJ[el] * a1;
     }
   }
 }

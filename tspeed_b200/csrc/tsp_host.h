@@ -10,6 +10,10 @@ namespace tsp {
 
 constexpr int kMaxN = 8;
 
+// Modal bases of the reference (ShapeFunctions.hpp): Dubiner<N> is
+// orthonormal, BoundaryAdapted<N> is not (its reference mass is dense).
+enum Basis : int { kDubiner = 0, kBoundaryAdapted = 1 };
+
 inline int np_of(int N) { return (N + 1) * (N + 2) / 2; }
 
 // Gauss-Legendre nodes/weights on [a, b] by Newton iteration
@@ -17,7 +21,7 @@ inline int np_of(int N) { return (N + 1) * (N + 2) / 2; }
 void gauleg(int n, double a, double b, double* x, double* w);
 
 // Jacobi polynomial P_n^{alpha,beta}(z) by the three-term recurrence of
-// ShapeFunctions.cpp:25-60.
+// ShapeFunctions.cpp:25-60; zero for n < 0 as there.
 double jacobi(int n, int alpha, int beta, double z);
 
 // Dubiner basis values at (csi, eta), ShapeFunctions_imp.hpp:33-34, ordered
@@ -26,6 +30,18 @@ double jacobi(int n, int alpha, int beta, double z);
 void dubiner_phi(int N, double csi, double eta, double* phi);
 // Reference gradients (d/dcsi, d/deta), ShapeFunctions_imp.hpp:35-50.
 void dubiner_grad(int N, double csi, double eta, double* gcsi, double* geta);
+
+// BoundaryAdapted basis values, ShapeFunctions_imp.hpp:55-118: the three
+// vertex modes (1-csi-eta, csi, eta), N-1 edge modes on each of the edges
+// eta = 0, csi = 0, csi + eta = 1, then the interior modes (j outer, i inner,
+// i + j < N). At eta = 1 the polynomial's limit is used (the reference's
+// formula is 0/0 there for degrees >= 3).
+void ba_phi(int N, double csi, double eta, double* phi);
+// Reference gradients of BoundaryAdapted<N>, eta < 1.
+void ba_grad(int N, double csi, double eta, double* gcsi, double* geta);
+
+void basis_phi(int basis, int N, double csi, double eta, double* phi);
+void basis_grad(int basis, int N, double csi, double eta, double* gcsi, double* geta);
 
 // Reference-element matrices of the factorised SIPG operator. All are
 // Np x Np, row-major [i][j]; w = quadrature weights of Gauss<N+1>
@@ -39,7 +55,12 @@ void dubiner_grad(int N, double csi, double eta, double* gcsi, double* geta);
 //   Ds[a][l]   = sum_k w_k g^a_l(k)_i b_l(k)_j         (traction trace, self)
 //   Dx[a][l][l'] = sum_k w_k g^a_l(k)_i b_l'(kk)_j     (traction trace, cross)
 struct RefTables {
-  int N = 0, Np = 0, Q = 0;
+  int N = 0, Np = 0, Q = 0, basis = kDubiner;
+  // Inverse of the reference mass M_ij = sum_q w_q phi_i phi_j
+  // (FESpace_imp.hpp:48-68): the identity for Dubiner, dense for
+  // BoundaryAdapted. [Np][Np] row-major.
+  std::vector<double> Minv;
+  std::vector<double> M;   // the reference mass itself
   std::vector<double> K;   // [2][2][Np][Np]
   std::vector<double> Ws;  // [3][Np][Np]
   std::vector<double> Wx;  // [3][3][Np][Np]
@@ -50,7 +71,14 @@ struct RefTables {
   std::vector<double> Ge;  // [3][2][Q][Np] reference gradients on edges
   std::vector<double> w1;  // [Q]
 };
-RefTables make_tables(int N);
+RefTables make_tables(int N, int basis = kDubiner);
+
+// Inverse of a symmetric positive definite n x n matrix (row-major) by
+// Cholesky factorisation; false if a pivot is not positive.
+bool spd_inverse(int n, const std::vector<double>& A, std::vector<double>* Ainv);
+// A = L L^T (Cholesky, L lower triangular, row-major) and L^-1; false if A
+// is not positive definite.
+bool cholesky(int n, const std::vector<double>& A, std::vector<double>* L, std::vector<double>* Linv);
 
 // Per-element geometry (Geometry.cpp:100-105, 125-132, 178-198): edge l is
 // opposite vertex l with endpoints (1,2), (2,0), (0,1).
@@ -76,7 +104,7 @@ void bsr_pattern(int32_t ne, const int32_t* neigh, std::vector<int32_t>* row_ptr
 // passing Triangle::intriangle (Geometry.cpp:112-118), reference coordinates
 // by invmap (Geometry.cpp:199-202) and basis values. Returns -1 if none.
 int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, double px,
-                     double py, double* phi);
+                     double py, double* phi, int basis = kDubiner);
 
 // Gmsh 2.2 ASCII reader (Mesh.cpp:174-257).
 bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,
@@ -89,8 +117,9 @@ void quadrature_points(int N, int32_t ne, const double* xy, const int32_t* tri, 
 
 // FESpace::transform (FESpace_imp.hpp:136-179): L2 projection of a vector
 // field given by its values at the quadrature points, fvals[ne][Q*Q][2], onto
-// the Dubiner modes, reference layout out[c*ne*Np + e*Np + i].
-void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out);
+// the modes of the basis, reference layout out[c*ne*Np + e*Np + i].
+void project(int N, int32_t ne, const double* xy, const int32_t* tri, const double* fvals, double* out,
+             int basis = kDubiner);
 
 // Force evaluation times (TimeAdvance.cpp:28,46 with M_last_time
 // accumulated in double, TimeAdvance.hpp:230).

@@ -1172,15 +1172,25 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
 // Shots [s0, s0+ns) of a device state u[(e*S + s)*2Np + c*Np + i] in the
 // reference's vector layout out[s - s0][c*ne*Np + e*Np + i]
 // (FESpace_imp.hpp:152-153): one thread per output value, coalesced writes.
+// Tinv (optional, [Np][Np] row-major): the state holds w = L^T u per element
+// and component; out = L^-T w, i.e. out_i = sum_j Tinv[j][i] w_j with
+// Tinv = L^-1.
 __global__ void k_state_to_ref(const double* __restrict__ u, int ne, int S, int Np, int s0, int ns,
-                               double* __restrict__ out) {
+                               double* __restrict__ out, const double* __restrict__ Tinv) {
   const long long per = 2ll * ne * Np;
   const long long n = per * ns;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
     const long long sl = o / per, rem = o - sl * per;
     const long long c = rem / ((long long)ne * Np), rem2 = rem - c * ne * Np;
     const long long e = rem2 / Np, i = rem2 - e * Np;
-    out[o] = u[(e * S + s0 + sl) * 2 * Np + c * Np + i];
+    const double* w = u + (e * S + s0 + sl) * 2 * Np + c * Np;
+    if (Tinv) {
+      double v = 0.0;
+      for (int j = int(i); j < Np; ++j) v = fma(Tinv[j * Np + i], w[j], v);  // L^-1 is lower triangular
+      out[o] = v;
+    } else {
+      out[o] = w[i];
+    }
   }
 }
 
@@ -1696,6 +1706,77 @@ __global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
     if (p.prec == 0) reinterpret_cast<double*>(p.out)[o] = v;
     else if (p.prec == 1) reinterpret_cast<float*>(p.out)[o] = float(v);
     else reinterpret_cast<__nv_bfloat16*>(p.out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
+  }
+}
+
+// Applies A (Np x Np, row-major) to every Np-segment of the rows (side 0:
+// B <- diag(A, A) B) or of the columns (side 1: B <- B diag(A, A)^T) of each
+// 2Np x 2Np block, in FP64, and stores the result in the storage type.
+// With A = L^-1, L the Cholesky factor of the reference mass of a
+// non-orthonormal basis, the two sides give L^-1 B L^-T, the operator in the
+// orthonormalised coordinates w = L^T u, where the per-element mass is again
+// rho_e detJ_e times the identity. in: FP64 blocks, column-major with column
+// pitch pin. Working in place (in == out, FP64, pout == pin) is allowed: each
+// chunk of columns (side 0) or rows (side 1) is read completely into shared
+// memory before any of it is written.
+constexpr int kFoldMaxNp = 45;  // Np of N = 8
+constexpr int kFoldVecs = 16;
+__global__ void __launch_bounds__(256) k_fold_basis(const double* in, int pin, int Np, const double* __restrict__ A,
+                                                    int side, int prec, int pout, void* out, float* scale) {
+  __shared__ double sA[kFoldMaxNp * kFoldMaxNp];
+  __shared__ double sv[2 * kFoldMaxNp * kFoldVecs];
+  __shared__ float s_max[8];
+  const int b = blockIdx.x, R = 2 * Np;
+  for (int t = threadIdx.x; t < Np * Np; t += blockDim.x) sA[t] = A[t];
+  const double* blk = in + size_t(b) * R * pin;
+  float amax = 0.0f, inv_sc = 1.0f;
+  for (int pass = (prec == 2 ? 0 : 1); pass < 2; ++pass) {
+    for (int v0 = 0; v0 < R; v0 += kFoldVecs) {
+      const int nv = min(kFoldVecs, R - v0);
+      __syncthreads();
+      // sv[vv][k]: entry k of vector v0 + vv (a column for side 0, a row for
+      // side 1); consecutive threads read consecutive addresses.
+      for (int t = threadIdx.x; t < nv * R; t += blockDim.x) {
+        if (side == 0) {
+          const int vv = t / R, k = t - vv * R;
+          sv[vv * R + k] = blk[size_t(v0 + vv) * pin + k];
+        } else {
+          const int k = t / nv, vv = t - k * nv;
+          sv[vv * R + k] = blk[size_t(k) * pin + v0 + vv];
+        }
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < nv * R; t += blockDim.x) {
+        const int vv = t / R, k = t - vv * R;
+        const int comp = k >= Np ? 1 : 0, i = k - comp * Np;
+        const double* vec = sv + vv * R + comp * Np;
+        double v = 0.0;
+        for (int j = 0; j < Np; ++j) v = fma(sA[i * Np + j], vec[j], v);
+        if (pass == 0) {
+          amax = fmaxf(amax, float(fabs(v)));
+        } else {
+          const int row = side == 0 ? k : v0 + vv, col = side == 0 ? v0 + vv : k;
+          const size_t o = size_t(b) * R * pout + size_t(col) * pout + row;
+          if (prec == 0) reinterpret_cast<double*>(out)[o] = v;
+          else if (prec == 1) reinterpret_cast<float*>(out)[o] = float(v);
+          else reinterpret_cast<__nv_bfloat16*>(out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
+        }
+      }
+    }
+    if (pass == 0) {
+      for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = amax;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        float m = 0.0f;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
+        const float scv = (m > 0.0f) ? exp2f(ceilf(log2f(m))) : 1.0f;  // as k_assemble
+        s_max[0] = scv;
+        scale[b] = scv;
+      }
+      __syncthreads();
+      inv_sc = 1.0f / s_max[0];
+    }
   }
 }
 
