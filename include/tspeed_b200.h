@@ -315,6 +315,34 @@ int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const i
 int tsp_project_basis(int32_t N, int32_t basis, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri,
                       const double* fvals, double* out);
 
+/* ---- Field output and error norms (FESpace_imp.hpp:70-133) ------------- */
+/* FESpace::field_out values of one shot's current displacement: the
+ * expansion at the reference points (0.2,0.2), (0.8,0.2), (0.2,0.8),
+ * (0.5,0.5) of every element, out[ne][4][2], evaluated on the device. */
+int tsp_field_values(tsp_handle* h, int32_t shot, double* out);
+/* Writes them as FESpace::field_out(fname, u, step) does: file
+ * fname + "u_" + step + ".field", one "valx valy" line per element and point,
+ * default iostream number formatting. */
+int tsp_write_field(tsp_handle* h, int32_t shot, const char* fname, int64_t step);
+/* FESpace::L2error(uex, u) of one shot's current displacement: exact values
+ * at the volume quadrature points (tsp_quadrature_points order),
+ * exact[ne][(N+1)^2][2]; per-element terms on the device, summed in element
+ * order on the host. The rule is the collapsed Gauss<N+1> of FESpace<N>
+ * (for BoundaryAdapted the reference integrates with Dunavant<2N>; both are
+ * exact for |u_h|^2 but differ for a non-polynomial uex). Needs a handle
+ * built from a mesh (TSP_ERR_UNSUPPORTED for tsp_create_from_blocks). */
+int tsp_l2_error(tsp_handle* h, int32_t shot, const double* exact, double* err);
+/* FESpace::points_out(fname): the physical positions of the field_out
+ * points, one "x y" line per element and point. */
+int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const char* fname);
+/* Basis values at reference points (for callers holding u on the host):
+ * rpts[npts][2] -> phi[npts][Np] (ShapeFunctions_imp.hpp). */
+int tsp_eval_basis(int32_t N, int32_t basis, int32_t npts, const double* rpts, double* phi);
+/* The volume rule on the reference triangle (collapsed Gauss<N+1>,
+ * QuadratureRule_imp.hpp:101-113): rpts[(N+1)^2][2], w[(N+1)^2]; either may
+ * be NULL. */
+int tsp_quadrature_rule(int32_t N, double* rpts, double* w);
+
 /* Host-side mesh services (Mesh.cpp). */
 /* Gmsh 2.2 ASCII reader (Mesh::Mesh, Mesh.cpp:174-257): counts first
  * (xy/tri/region NULL), then data. region = elementary tag. */

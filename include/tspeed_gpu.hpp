@@ -118,6 +118,72 @@ class FESpace {
                             vals.data(), out.data()));
     return out;
   }
+  // FESpace::points_out (FESpace_imp.hpp:70-84).
+  void points_out(const std::string& fname) const {
+    check(tsp_points_out(int32_t(mesh_->nverts()), mesh_->xy().data(), int32_t(mesh_->ne()), mesh_->tri().data(),
+                         fname.c_str()));
+  }
+  // FESpace::field_out (FESpace_imp.hpp:85-105) of a host vector uh
+  // (reference layout); LeapFrog::field_out evaluates the device state.
+  void field_out(const std::string& fname, const std::vector<double>& uh, unsigned step) const {
+    static const double pts[8] = {0.2, 0.2, 0.8, 0.2, 0.2, 0.8, 0.5, 0.5};
+    const size_t Np = nln(), ne = mesh_->ne();
+    std::vector<double> V(4 * Np);
+    check(tsp_eval_basis(N_, basis_, 4, pts, V.data()));
+    std::ofstream o(fname + "u_" + std::to_string(step) + ".field");
+    for (size_t e = 0; e < ne; ++e)
+      for (int q = 0; q < 4; ++q) {
+        double vx = 0.0, vy = 0.0;
+        for (size_t i = 0; i < Np; ++i) {
+          vx += V[q * Np + i] * uh[e * Np + i];
+          vy += V[q * Np + i] * uh[ne * Np + e * Np + i];
+        }
+        o << vx << " " << vy << std::endl;
+      }
+  }
+  // FESpace::L2error (FESpace_imp.hpp:107-133) of a host vector uh, on the
+  // collapsed Gauss<N+1> rule.
+  double L2error(const std::function<std::array<double, 2>(double, double)>& uex,
+                 const std::vector<double>& uh) const {
+    const int32_t ne = int32_t(mesh_->ne()), nq = (N_ + 1) * (N_ + 1);
+    const size_t Np = nln();
+    std::vector<double> r(2 * size_t(nq)), w(nq), B(size_t(nq) * Np), pts(size_t(ne) * nq * 2);
+    check(tsp_quadrature_rule(N_, r.data(), w.data()));
+    check(tsp_eval_basis(N_, basis_, nq, r.data(), B.data()));
+    check(tsp_quadrature_points(N_, int32_t(mesh_->nverts()), mesh_->xy().data(), ne, mesh_->tri().data(),
+                                pts.data()));
+    const std::vector<double> det = detJ();
+    double err = 0.0;
+    for (int32_t e = 0; e < ne; ++e) {
+      double loc = 0.0;
+      for (int32_t q = 0; q < nq; ++q) {
+        double ax = 0.0, ay = 0.0;
+        for (size_t i = 0; i < Np; ++i) {
+          ax += B[q * Np + i] * uh[size_t(e) * Np + i];
+          ay += B[q * Np + i] * uh[size_t(ne) * Np + size_t(e) * Np + i];
+        }
+        const size_t k = size_t(e) * nq + q;
+        const std::array<double, 2> f = uex(pts[2 * k], pts[2 * k + 1]);
+        loc += ((ax - f[0]) * (ax - f[0]) + (ay - f[1]) * (ay - f[1])) * w[q];
+      }
+      err += loc * det[e];
+    }
+    return std::sqrt(err);
+  }
+  // Signed Jacobian determinants (Geometry.cpp:188-192).
+  std::vector<double> detJ() const {
+    const size_t ne = mesh_->ne();
+    std::vector<double> d(ne);
+    const std::vector<double>& xy = mesh_->xy();
+    const std::vector<int32_t>& t = mesh_->tri();
+    for (size_t e = 0; e < ne; ++e) {
+      const double* p0 = &xy[2 * size_t(t[3 * e])];
+      const double* p1 = &xy[2 * size_t(t[3 * e + 1])];
+      const double* p2 = &xy[2 * size_t(t[3 * e + 2])];
+      d[e] = (p1[0] - p0[0]) * (p2[1] - p0[1]) - (p2[0] - p0[0]) * (p1[1] - p0[1]);
+    }
+    return d;
+  }
 
  private:
   Mesh_ptr mesh_;
@@ -242,6 +308,23 @@ class LeapFrog {
     return uh_;
   }
   const std::vector<double>& get_uh() { return u(); }
+  // Xh->field_out(fname, u(), step) and Xh->L2error(uex, u()) evaluated on
+  // the device state.
+  void field_out(const std::string& fname, unsigned step) { check(tsp_write_field(h_, 0, fname.c_str(), step), h_); }
+  double L2error(const std::function<std::array<double, 2>(double, double)>& uex) {
+    const Mesh& m = *Xh_->mesh();
+    const int32_t ne = int32_t(m.ne()), nq = (Xh_->degree() + 1) * (Xh_->degree() + 1);
+    std::vector<double> pts(size_t(ne) * nq * 2), ex(size_t(ne) * nq * 2);
+    check(tsp_quadrature_points(Xh_->degree(), int32_t(m.nverts()), m.xy().data(), ne, m.tri().data(), pts.data()));
+    for (size_t k = 0; k < size_t(ne) * nq; ++k) {
+      const std::array<double, 2> f = uex(pts[2 * k], pts[2 * k + 1]);
+      ex[2 * k] = f[0];
+      ex[2 * k + 1] = f[1];
+    }
+    double err = 0.0;
+    check(tsp_l2_error(h_, 0, ex.data(), &err), h_);
+    return err;
+  }
   // TimeAdvance::eval_receivers (TimeAdvance.cpp:68-79): the device samples
   // every step; this records which steps are written out.
   void eval_receivers() {

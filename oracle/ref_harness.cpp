@@ -14,7 +14,11 @@
 //   * the mesh neighbour tables (Mesh.cpp:33-128),
 //   * source / receiver location (Receivers_imp.hpp:34-51),
 //   * displacement snapshots and receiver samples of the leap-frog loop
-//     (TimeAdvance.cpp:24-59).
+//     (TimeAdvance.cpp:24-59),
+//   * the FESpace services around the loop: transform of a fixed field
+//     (FESpace_imp.hpp:136-179), L2error (FESpace_imp.hpp:107-133) of that
+//     projection and of the final displacement, and the text outputs
+//     field_out / points_out (FESpace_imp.hpp:70-106) of the final step.
 //
 // LeapFrogP re-forms B with the requested penalty. In the reference, B is built
 // in the LeapFrog constructor with the default M_penalty(2)
@@ -32,6 +36,7 @@
 #include "TSPEED.hpp"
 
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -257,8 +262,30 @@ int run_space(const Args& a) {
   if (!(a.u_every > 0 && steps % a.u_every == 0)) snap(steps);
   std::fclose(fu);
   std::fclose(fs);
-  std::printf("{\"ne\": %u, \"Np\": %u, \"steps\": %ld, \"last_time\": %.17g, \"setup_s\": %.6f, \"loop_s\": %.6f}\n",
-              ne, nln, steps, TA.last_time(), setup_s, loop_s);
+
+  // ---- FESpace services ----
+  // The projected field: smooth for the Dubiner space (transform and L2error
+  // integrate with Gauss<N+1> there); linear for BoundaryAdapted, whose
+  // Dunavant<2N> rule then integrates every product exactly as well.
+  const bool ba = !S::is_orthonormal;
+  auto field = [ba](double x, double y) {
+    if (ba) return std::array<double, 2>{{1e-3 + 2e-6 * x - 3e-6 * y, -2e-3 + 1e-6 * x + 4e-6 * y}};
+    return std::array<double, 2>{{std::sin(x / 97.0) * std::cos(y / 61.0), 1e-6 * x * y}};
+  };
+  const Eigen::VectorXd proj = Xh->transform(field);
+  {
+    std::FILE* f = std::fopen((a.out + ".proj.bin").c_str(), "wb");
+    if (!f) die("cannot open output");
+    wr(f, proj.data(), size_t(proj.size()));
+    std::fclose(f);
+  }
+  const double l2_proj = Xh->L2error(field, proj);
+  const double l2_u = Xh->L2error([](double, double) { return std::array<double, 2>{{0.0, 0.0}}; }, TA.u());
+  Xh->field_out(a.out + ".", TA.u(), unsigned(steps));
+  Xh->points_out(a.out + ".points");
+  std::printf("{\"ne\": %u, \"Np\": %u, \"steps\": %ld, \"last_time\": %.17g, \"setup_s\": %.6f, \"loop_s\": %.6f, "
+              "\"l2_proj\": %.17g, \"l2_u\": %.17g}\n",
+              ne, nln, steps, TA.last_time(), setup_s, loop_s, l2_proj, l2_u);
   return 0;
 }
 

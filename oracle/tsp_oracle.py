@@ -477,6 +477,69 @@ def transform(sp: Space, xy, tri, geo: Geom, fun):
     return np.concatenate([(rx / geo.detJ[:, None]).ravel(), (ry / geo.detJ[:, None]).ravel()])
 
 
+# Reference points of FESpace::field_out / points_out (FESpace_imp.hpp:31-34,
+# 70-84): three near the vertices and the midpoint of the long edge.
+FIELD_POINTS = np.array([[0.2, 0.2], [0.8, 0.2], [0.2, 0.8], [0.5, 0.5]])
+
+
+def field_values(sp: Space, u, ne: int) -> np.ndarray:
+    """FESpace::field_out values (FESpace_imp.hpp:85-105): the expansion of
+    each component at FIELD_POINTS, [ne, 4, 2]."""
+    V = basis_phi(sp.N, sp.basis, FIELD_POINTS[:, 0], FIELD_POINTS[:, 1])  # [Np, 4]
+    ux = u[:ne * sp.Np].reshape(ne, sp.Np) @ V
+    uy = u[ne * sp.Np:].reshape(ne, sp.Np) @ V
+    return np.stack([ux, uy], -1)
+
+
+def gformat(v: float) -> str:
+    """A double as std::ostream prints it by default (precision 6, %g)."""
+    return "%g" % v
+
+
+def field_text(vals) -> str:
+    """The lines FESpace::field_out writes: "valx valy" per element and point."""
+    return "".join(f"{gformat(x)} {gformat(y)}\n" for x, y in np.asarray(vals).reshape(-1, 2))
+
+
+def points_text(xy, tri) -> str:
+    """FESpace::points_out (FESpace_imp.hpp:70-84): Triangle::map of
+    FIELD_POINTS (p0 + J p^, Geometry.cpp:203-207) for every element."""
+    lines = []
+    for t in tri:
+        p0, p1, p2 = xy[t[0]], xy[t[1]], xy[t[2]]
+        for a, b in FIELD_POINTS:
+            x = p0[0] + ((p1[0] - p0[0]) * a + (p2[0] - p0[0]) * b)
+            y = p0[1] + ((p1[1] - p0[1]) * a + (p2[1] - p0[1]) * b)
+            lines.append(f"{gformat(x)} {gformat(y)}\n")
+    return "".join(lines)
+
+
+def l2_error(sp: Space, geo: Geom, u, exact) -> float:
+    """FESpace::L2error (FESpace_imp.hpp:107-133): sqrt(sum_e detJ_e
+    sum_q |u_h(x_q) - u(x_q)|^2 w_q), elements and points in order; exact is
+    [ne, nq, 2] at the volume quadrature points."""
+    ne, Np = geo.detJ.shape[0], sp.Np
+    ax = u[:ne * Np].reshape(ne, Np) @ sp.B.T
+    ay = u[ne * Np:].reshape(ne, Np) @ sp.B.T
+    err = 0.0
+    for e in range(ne):
+        loc = 0.0
+        for q in range(sp.B.shape[0]):
+            dx, dy = ax[e, q] - exact[e, q, 0], ay[e, q] - exact[e, q, 1]
+            loc += (dx * dx + dy * dy) * sp.rule.w2d[q]
+        err += loc * geo.detJ[e]
+    return float(np.sqrt(err))
+
+
+def quadrature_points(sp: Space, xy, tri) -> np.ndarray:
+    """Physical volume quadrature points [ne, nq, 2] (Triangle::map)."""
+    p = xy[tri]
+    n2 = sp.rule.nodes2d
+    X = p[:, 0, 0][:, None] + ((p[:, 1, 0] - p[:, 0, 0])[:, None] * n2[None, :, 0] + (p[:, 2, 0] - p[:, 0, 0])[:, None] * n2[None, :, 1])
+    Y = p[:, 0, 1][:, None] + ((p[:, 1, 1] - p[:, 0, 1])[:, None] * n2[None, :, 0] + (p[:, 2, 1] - p[:, 0, 1])[:, None] * n2[None, :, 1])
+    return np.stack([X, Y], -1)
+
+
 # --------------------------------------------------------------------------
 # Point location, sources, receivers.
 # --------------------------------------------------------------------------

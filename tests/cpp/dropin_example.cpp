@@ -65,6 +65,13 @@ int main(int argc, char** argv) {
     double s = 0;
     for (double v : u) s += v * v;
     std::printf("steps %d norm %.17g\n", steps, std::sqrt(s));
+    // FESpace outputs (FESpace_imp.hpp:70-133): on the host from u, and from
+    // the device state.
+    auto zero = [](double, double) { return std::array<double, 2>{{0.0, 0.0}}; };
+    Xh->points_out(out + ".points");
+    Xh->field_out(out + ".host.", u, unsigned(steps));
+    TA.field_out(out + ".dev.", unsigned(steps));
+    std::printf("l2 %.17g %.17g\n", Xh->L2error(zero, u), TA.L2error(zero));
   } catch (const Error& e) {
     std::fprintf(stderr, "tspeed_gpu error %d: %s\n", e.code(), e.what());
     return 1;

@@ -9,6 +9,10 @@ outputs as .npz. Rebuild with:
 
 Cases named g_ba_* use the reference's BoundaryAdapted space
 (FESpace<N, Dunavant<2N>, BoundaryAdapted<N>>, Examples/src/Lamb.cpp:26).
+Each case also holds the reference's FESpace services: transform of a fixed
+field (proj), L2error of that projection (l2_proj) and of the final
+displacement (l2_u), and the text written by field_out / points_out for the
+final step (field_txt / points_txt, bytes).
 """
 from __future__ import annotations
 
@@ -100,11 +104,15 @@ def run_case(name, c, tmp):
     snaps = {int(np.frombuffer(u, np.int64, 1, i)[0]): np.frombuffer(u, np.float64, 2 * ne * Np, i + 8)
              for i in range(0, len(u), rec)}
     seis = np.fromfile(out + ".seis.bin", dtype=np.float64).reshape(c["nsteps"], nr, 2)
+    proj = np.fromfile(out + ".proj.bin", dtype=np.float64)
+    field_txt = np.frombuffer(open(out + ".u_%d.field" % c["nsteps"], "rb").read(), np.uint8)
+    points_txt = np.frombuffer(open(out + ".points", "rb").read(), np.uint8)
     d = dict(xy=m.xy, tri=m.tri, region=m.region, lam=lam, mu=mu, rho=rho, N=c["N"], penalty=c["penalty"],
              dt=c["dt"], nsteps=c["nsteps"], src=np.array(c["src"]), ricker=np.array(c["ricker"]),
              rcv=np.array(rcv), neigh=nb[:, :3], nedge=nb[:, 3:], detJ=geo[:, 0], minv=minv, src_elem=src_elem,
              src_phi=src_phi, rcv_elem=np.array(rcv_elem), rcv_phi=np.array(rcv_phi), seis=seis,
-             u_first=snaps[1], u_final=snaps[c["nsteps"]], last_time=info["last_time"])
+             u_first=snaps[1], u_final=snaps[c["nsteps"]], last_time=info["last_time"],
+             proj=proj, l2_proj=info["l2_proj"], l2_u=info["l2_u"], field_txt=field_txt, points_txt=points_txt)
     if c.get("basis", "dubiner") != "dubiner":
         d["basis"] = c["basis"]
         d["minv_ref"] = minv_ref

@@ -28,3 +28,21 @@ def oracle_setup(g):
 def rel(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def golden_field(g):
+    """The field the golden generator projects (tests/golden/make_golden.py
+    runs the reference harness, oracle/ref_harness.cpp, which defines it):
+    smooth for Dubiner cases, linear for BoundaryAdapted ones."""
+    if "basis" in g and str(g["basis"]) == "ba":
+        return lambda x, y: (1e-3 + 2e-6 * x - 3e-6 * y + 0 * x, -2e-3 + 1e-6 * x + 4e-6 * y + 0 * x)
+    return lambda x, y: (np.sin(x / 97.0) * np.cos(y / 61.0), 1e-6 * x * y)
+
+
+def l2_proj_tol(g):
+    """Absolute tolerance on the golden projection error: rounding of the
+    field's values (|f| <= 1 on a domain of area A) dominates,
+    1e-13 * sqrt(A) * max|f|."""
+    xy = g["xy"]
+    area = float(np.ptp(xy[:, 0]) * np.ptp(xy[:, 1]))
+    return 1e-13 * np.sqrt(area) * 1.0 + 1e-12 * float(g["l2_proj"])

@@ -41,3 +41,14 @@ def test_cpp_dropin_matches_reference_golden(tmp_path):
     assert seis.shape == g["seis"].shape
     ok = np.isfinite(g["seis"])
     assert rel(seis[ok], g["seis"][ok]) < 1e-12
+    # FESpace::points_out / field_out / L2error, host and device forms.
+    n = int(g["nsteps"])
+    assert (tmp_path / "out.points").read_bytes() == bytes(g["points_txt"])
+    ref = np.array([[float(v) for v in ln.split()] for ln in bytes(g["field_txt"]).decode().splitlines()])
+    scale = np.abs(ref).max()
+    for form in ("host", "dev"):
+        got = np.loadtxt(str(tmp_path / f"out.{form}.u_{n}.field"))
+        assert got.shape == ref.shape
+        assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-11 * scale)
+    l2 = [float(v) for v in res.stdout.splitlines()[1].split()[1:]]
+    assert abs(l2[0] / float(g["l2_u"]) - 1) < 1e-12 and abs(l2[1] / float(g["l2_u"]) - 1) < 1e-12

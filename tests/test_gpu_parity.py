@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import tsp_oracle as O
-from helpers import oracle_setup, rel
+from helpers import golden_field, l2_proj_tol, oracle_setup, rel
 from tspeed_b200 import capi
 from tspeed_b200 import workloads as W
 
@@ -514,3 +514,54 @@ def test_boundary_adapted_checkpoint_resume_and_initial_state():
         assert rel(b.u(0), a.u(0)) < 1e-12 and rel(b.u(1), a.u(1)) < 1e-12
         assert rel(b.u_all(), a.u_all()) < 1e-12
         assert rel(a.u_all()[1], a.u(1)) < 1e-15  # device and host maps, same L^-T
+
+
+def _parse_pairs(txt):
+    return np.array([[float(v) for v in ln.split()] for ln in txt.splitlines()])
+
+
+def test_golden_field_output_and_l2_error(golden, tmp_path):
+    """FESpace::field_out / L2error / transform of the reference, through the
+    device state: the field file written after the golden run against the
+    reference's own file (printed to 6 digits; values that are rounding noise
+    of the run may differ in their digits, so the comparison is numeric at
+    the printed precision relative to the field's scale), L2error of the final
+    displacement, and L2error of the reference's projection loaded as the
+    initial state."""
+    g = golden
+    n = int(g["nsteps"])
+    with sim_from_golden(g) as s:
+        s.first_step()
+        s.run(n - 1)
+        s.write_field(str(tmp_path / "g."), n)
+        txt = (tmp_path / ("g.u_%d.field" % n)).read_text()
+        vals = s.field_values()
+        nq = (int(g["N"]) + 1) ** 2
+        l2u = s.l2_error(np.zeros((g["tri"].shape[0], nq, 2)))
+        s.set_initial(0, g["proj"], None)
+        pts = capi.quadrature_points(int(g["N"]), g["xy"], g["tri"])
+        fx, fy = golden_field(g)(pts[..., 0], pts[..., 1])
+        l2p = s.l2_error(np.stack([fx, fy], -1))
+    ref = _parse_pairs(bytes(g["field_txt"]).decode())
+    got = _parse_pairs(txt)
+    scale = np.abs(ref).max()
+    same = sum(a == b for a, b in zip(txt.splitlines(), bytes(g["field_txt"]).decode().splitlines()))
+    print(g["name"], "field lines identical", same, "/", len(ref), "l2u", abs(l2u / float(g["l2_u"]) - 1),
+          "l2p", abs(l2p - float(g["l2_proj"])))
+    assert got.shape == ref.shape
+    assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-11 * scale)
+    assert np.allclose(vals.reshape(-1, 2), got, rtol=1e-5, atol=1e-11 * scale)
+    _, tn = tols(g)
+    assert abs(l2u / float(g["l2_u"]) - 1) < tn
+    assert abs(l2p - float(g["l2_proj"])) <= l2_proj_tol(g)
+
+
+def test_l2_error_needs_the_mesh():
+    g = __import__("conftest").load_golden("g_n2_layers")
+    rphi = np.nan_to_num(g["rcv_phi"])
+    with capi.Simulation.from_blocks(g["row_ptr"], g["col"], g["blocks"], g["minv"], [int(g["src_elem"])],
+                                     g["src_phi"][None], g["rcv_elem"], rphi) as s:
+        with pytest.raises(capi.TspError) as e:
+            s.l2_error(np.zeros((g["tri"].shape[0], 9, 2)))
+        assert e.value.code == -9
+        assert s.field_values().shape == (g["tri"].shape[0], 4, 2)

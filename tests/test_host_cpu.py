@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import tsp_oracle as O
+from helpers import golden_field
 from tspeed_b200 import capi
 from tspeed_b200 import workloads as W
 
@@ -131,3 +132,35 @@ def test_projection_reproduces_polynomials_of_degree_N(basis):
     vy = uh[ne * Np:].reshape(ne, Np) @ sp.B.T
     assert np.abs(vx - fx).max() < 1e-10 * max(1.0, np.abs(fx).max())
     assert np.abs(vy - fy).max() < 1e-10 * max(1.0, np.abs(fy).max())
+
+
+def test_points_out_matches_reference_bytes(golden, tmp_path):
+    """FESpace::points_out text of the reference, byte for byte."""
+    f = tmp_path / "pts"
+    capi.points_out(golden["xy"], golden["tri"], str(f))
+    assert f.read_bytes() == bytes(golden["points_txt"])
+
+
+def test_projection_matches_reference_golden(golden):
+    """tsp_project_basis against the reference's own FESpace::transform."""
+    g = golden
+    basis = str(g["basis"]) if "basis" in g else "dubiner"
+    N = int(g["N"])
+    pts = capi.quadrature_points(N, g["xy"], g["tri"])
+    fx, fy = golden_field(g)(pts[..., 0], pts[..., 1])
+    got = capi.project(N, g["xy"], g["tri"], np.stack([fx, fy], -1), basis=basis)
+    tol = 1e-13 if basis == "dubiner" else 1e-11  # cond(M_ref) for BoundaryAdapted
+    assert np.abs(got - g["proj"]).max() / np.abs(g["proj"]).max() < tol
+
+
+@pytest.mark.parametrize("basis", ["dubiner", "ba"])
+@pytest.mark.parametrize("N", [1, 4, 8])
+def test_eval_basis_and_quadrature_rule_match_oracle(N, basis):
+    sp = O.make_space(N, basis)
+    r, w = capi.quadrature_rule(N)
+    assert np.abs(r - sp.rule.nodes2d).max() < 1e-15 and np.abs(w - sp.rule.w2d).max() < 1e-16
+    rng = np.random.default_rng(N)
+    c = rng.random(30)
+    e = rng.random(30) * (1 - c)
+    phi = capi.eval_basis(N, np.stack([c, e], -1), basis=basis)
+    assert np.abs(phi - O.basis_phi(N, basis, c, e).T).max() < 1e-12

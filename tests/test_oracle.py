@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 import tsp_oracle as O
-from helpers import oracle_setup, rel
+from helpers import golden_field, l2_proj_tol, oracle_setup, rel
 
 
 def test_neighbours_match_reference(golden):
@@ -143,3 +143,32 @@ def test_seismograms_do_not_depend_on_the_basis(N):
         out[basis] = seis
     assert (np.abs(out["dubiner"][-1]) > 0).all()
     assert rel(out["ba"], out["dubiner"]) < 1e-12
+
+
+def test_field_and_points_output_match_reference_bytes(golden):
+    """FESpace::field_out / points_out text of the reference (final step),
+    byte for byte (FESpace_imp.hpp:70-105)."""
+    g = golden
+    o = oracle_setup(g)
+    ne = g["tri"].shape[0]
+    assert O.field_text(O.field_values(o["sp"], g["u_final"], ne)) == bytes(g["field_txt"]).decode()
+    assert O.points_text(g["xy"], g["tri"]) == bytes(g["points_txt"]).decode()
+
+
+def test_projection_and_l2_error_match_reference(golden):
+    """FESpace::transform of the generator's field and FESpace::L2error of
+    that projection and of the final displacement (FESpace_imp.hpp:107-179)."""
+    g = golden
+    o = oracle_setup(g)
+    ne, tri = g["tri"].shape[0], g["tri"].astype(np.int64)
+    fun = golden_field(g)
+    proj = O.transform(o["sp"], g["xy"], tri, o["geo"], fun)
+    tol = 1e-13 if o["basis"] == "dubiner" else 1e-11  # cond(M_ref) for BoundaryAdapted
+    assert np.abs(proj - g["proj"]).max() / np.abs(g["proj"]).max() < tol
+    qp = O.quadrature_points(o["sp"], g["xy"], tri)
+    fx, fy = fun(qp[..., 0], qp[..., 1])
+    l2p = O.l2_error(o["sp"], o["geo"], g["proj"], np.stack([fx, fy], -1))
+    assert abs(l2p - float(g["l2_proj"])) <= l2_proj_tol(g)
+    nq = o["sp"].B.shape[0]
+    l2u = O.l2_error(o["sp"], o["geo"], g["u_final"], np.zeros((ne, nq, 2)))
+    assert abs(l2u - float(g["l2_u"])) <= 1e-14 * float(g["l2_u"])

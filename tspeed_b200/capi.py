@@ -92,6 +92,12 @@ SIGNATURES = {
     "tsp_project": (C.c_int, [C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
     "tsp_project_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int32, _ip, _dp, _dp]),
     "tsp_get_ref_invmass": (C.c_int, [C.c_void_p, _ip, _dp]),
+    "tsp_field_values": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "tsp_write_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int64]),
+    "tsp_l2_error": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
+    "tsp_points_out": (C.c_int, [C.c_int32, _dp, C.c_int32, _ip, C.c_char_p]),
+    "tsp_eval_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
+    "tsp_quadrature_rule": (C.c_int, [C.c_int32, _dp, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
     "tsp_mesh_neighbours": (C.c_int, [C.c_int32, _ip, _ip, _ip]),
 }
@@ -175,6 +181,27 @@ def project(N: int, xy, tri, fvals, basis: str = "dubiner"):
     _check(lib().tsp_project_basis(N, TSP_BASIS[basis], xy.shape[0], _d(xy), tri.shape[0], _i(tri), _d(fvals),
                                    _d(out)))
     return out
+
+
+def points_out(xy, tri, fname: str):
+    """FESpace::points_out: the physical field_out points of every element."""
+    xy, tri = _f64(xy), _i32(tri)
+    _check(lib().tsp_points_out(xy.shape[0], _d(xy), tri.shape[0], _i(tri), os.fsencode(fname)))
+
+
+def eval_basis(N: int, rpts, basis: str = "dubiner"):
+    """Basis values phi[npts][Np] at reference points rpts[npts][2]."""
+    rpts = _f64(np.asarray(rpts, dtype=np.float64).reshape(-1, 2))
+    out = np.zeros((rpts.shape[0], (N + 1) * (N + 2) // 2))
+    _check(lib().tsp_eval_basis(N, TSP_BASIS[basis], rpts.shape[0], _d(rpts), _d(out)))
+    return out
+
+
+def quadrature_rule(N: int):
+    """Collapsed Gauss<N+1> volume rule: reference nodes [(N+1)^2, 2], weights."""
+    r, w = np.zeros(((N + 1) ** 2, 2)), np.zeros((N + 1) ** 2)
+    _check(lib().tsp_quadrature_rule(N, _d(r), _d(w)))
+    return r, w
 
 
 def force_times(dt: float, n: int):
@@ -313,6 +340,23 @@ class Simulation:
         return out
 
     # ---- outputs ----
+    def field_values(self, shot: int = 0):
+        """FESpace::field_out values of the current displacement, [ne, 4, 2]."""
+        out = np.zeros((self.ne, 4, 2))
+        _check(lib().tsp_field_values(self._h, shot, _d(out)), self._h)
+        return out
+
+    def write_field(self, fname: str, step: int, shot: int = 0):
+        """FESpace::field_out(fname, u, step): writes fname + "u_<step>.field"."""
+        _check(lib().tsp_write_field(self._h, shot, os.fsencode(fname), step), self._h)
+
+    def l2_error(self, exact, shot: int = 0) -> float:
+        """FESpace::L2error against exact values at quadrature_points()."""
+        exact = _f64(exact)
+        err = C.c_double()
+        _check(lib().tsp_l2_error(self._h, shot, _d(exact), C.byref(err)), self._h)
+        return err.value
+
     def u(self, shot: int = 0):
         out = np.zeros(2 * self.ne * self.Np)
         _check(lib().tsp_get_u(self._h, shot, _d(out)), self._h)

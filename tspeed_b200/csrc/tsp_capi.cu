@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -43,6 +44,9 @@ struct tsp_handle {
   int basis = tsp::kDubiner;
   std::vector<double> minv_ref, lref, lref_inv;
   double* d_lref_inv = nullptr;
+  // Signed element determinants (handles built from a mesh; empty for
+  // tsp_create_from_blocks), for tsp_l2_error.
+  std::vector<double> detJ;
   // operator
   int* d_row_ptr = nullptr;
   int* d_col = nullptr;
@@ -814,6 +818,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
                                 "Matrices_imp.hpp:186-189 would be non-positive");
       return create_error_from(h, TSP_ERR_MESH);
     }
+  h->detJ = g.detJ;
   std::vector<int32_t> neigh(size_t(P->ne) * 3), nedge(size_t(P->ne) * 3);
   std::string err;
   if (!tsp::build_neighbours(P->ne, P->tri, neigh.data(), nedge.data(), &err)) {
@@ -1625,6 +1630,146 @@ int tsp_project_basis(int32_t N, int32_t basis, int32_t nverts, const double* xy
 int tsp_project(int32_t N, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const double* fvals,
                 double* out) {
   return tsp_project_basis(N, TSP_BASIS_DUBINER, nverts, xy, ne, tri, fvals, out);
+}
+
+namespace {
+
+// Basis values at reference points in the device's coordinates: T[q][j] =
+// phi_j(r_q) for Dubiner, (L^-1 phi(r_q))_j for a non-orthonormal basis
+// (u_h = phi^T u = (L^-1 phi)^T w).
+std::vector<double> device_basis_table(const tsp_handle* h, int npt, const double* rc, const double* re) {
+  std::vector<double> T(size_t(npt) * h->Np);
+  for (int q = 0; q < npt; ++q) tsp::basis_phi(h->basis, h->N, rc[q], re[q], &T[size_t(q) * h->Np]);
+  if (!h->lref_inv.empty()) map_vectors(h->lref_inv, false, h->Np, T.data(), npt);
+  return T;
+}
+
+int field_values(tsp_handle* h, int shot, std::vector<double>* vals) {
+  double rc[4], re[4];
+  for (int q = 0; q < 4; ++q) {
+    rc[q] = tsp::kFieldPoints[q][0];
+    re[q] = tsp::kFieldPoints[q][1];
+  }
+  const std::vector<double> T = device_basis_table(h, 4, rc, re);
+  int rc_ = TSP_OK;
+  double *dT = nullptr, *dout = nullptr;
+  const size_t n = size_t(h->ne) * 8;
+  if ((rc_ = upload(h, &dT, T.data(), T.size())) || (rc_ = dalloc(h, &dout, n))) return rc_;
+  tsp::k_eval_points<<<1184, 256, 0, h->stream>>>(h->d_U[h->cur], h->ne, h->S, h->Np, shot, dT, 4, dout);
+  vals->resize(n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vals->data(), dout, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  dfree(h, dT);
+  dfree(h, dout);
+  if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("field values: ") + cudaGetErrorString(e));
+  return TSP_OK;
+}
+
+}  // namespace
+
+int tsp_field_values(tsp_handle* h, int32_t shot, double* out) {
+  if (!h || !out) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  std::vector<double> v;
+  if ((rc = field_values(h, shot, &v))) return rc;
+  std::copy(v.begin(), v.end(), out);
+  return check_device_error(h);
+}
+
+int tsp_write_field(tsp_handle* h, int32_t shot, const char* fname, int64_t step) {
+  if (!h || !fname || step < 0) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  std::vector<double> v;
+  if ((rc = field_values(h, shot, &v))) return rc;
+  if ((rc = check_device_error(h))) return rc;
+  // The file name and line format of FESpace::field_out (FESpace_imp.hpp:89-103).
+  const std::string path = std::string(fname) + "u_" + std::to_string(step) + ".field";
+  std::ofstream f(path);
+  if (!f.is_open()) return fail(h, TSP_ERR_ARG, "cannot open " + path);
+  for (size_t i = 0; i < v.size(); i += 2) f << v[i] << " " << v[i + 1] << std::endl;
+  if (!f.good()) return fail(h, TSP_ERR_ARG, "write failed: " + path);
+  return TSP_OK;
+}
+
+int tsp_l2_error(tsp_handle* h, int32_t shot, const double* exact, double* err) {
+  if (!h || !exact || !err) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  if (h->detJ.empty()) return fail(h, TSP_ERR_UNSUPPORTED, "the L2 error needs the mesh (handle built from blocks)");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  std::vector<double> c, e, w;
+  tsp::volume_rule(h->N, &c, &e, &w);
+  const int nq = int(w.size());
+  const std::vector<double> T = device_basis_table(h, nq, c.data(), e.data());
+  double *dT = nullptr, *dw = nullptr, *dJ = nullptr, *dex = nullptr, *dout = nullptr;
+  if ((rc = upload(h, &dT, T.data(), T.size())) || (rc = upload(h, &dw, w.data(), w.size())) ||
+      (rc = upload(h, &dJ, h->detJ.data(), h->detJ.size())) ||
+      (rc = upload(h, &dex, exact, size_t(h->ne) * nq * 2)) || (rc = dalloc(h, &dout, size_t(h->ne)))) {
+    for (void* q : {(void*)dT, (void*)dw, (void*)dJ, (void*)dex, (void*)dout}) dfree(h, q);
+    return rc;
+  }
+  tsp::k_l2_local<<<(h->ne + 255) / 256, 256, 0, h->stream>>>(h->d_U[h->cur], h->ne, h->S, h->Np, shot, dT, dw, nq, dJ,
+                                                               dex, dout);
+  std::vector<double> loc(h->ne);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(loc.data(), dout, loc.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+  for (void* q : {(void*)dT, (void*)dw, (void*)dJ, (void*)dex, (void*)dout}) dfree(h, q);
+  if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("L2 error: ") + cudaGetErrorString(ce));
+  double s = 0.0;
+  for (double v : loc) s += v;
+  *err = std::sqrt(s);
+  return check_device_error(h);
+}
+
+int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const char* fname) {
+  if (nverts <= 0 || ne <= 0 || !xy || !tri || !fname) return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_points_out");
+  for (int32_t i = 0; i < 3 * ne; ++i)
+    if (tri[i] < 0 || tri[i] >= nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  std::ofstream f(fname);
+  if (!f.is_open()) return fail(nullptr, TSP_ERR_ARG, std::string("cannot open ") + fname);
+  // Triangle::map(p) = p0 + J p (Geometry.cpp:203-207), J = [p1 - p0 | p2 - p0].
+  for (int32_t el = 0; el < ne; ++el) {
+    const double* p0 = xy + 2 * size_t(tri[3 * size_t(el)]);
+    const double* p1 = xy + 2 * size_t(tri[3 * size_t(el) + 1]);
+    const double* p2 = xy + 2 * size_t(tri[3 * size_t(el) + 2]);
+    for (int q = 0; q < 4; ++q) {
+      const double a = tsp::kFieldPoints[q][0], b = tsp::kFieldPoints[q][1];
+      f << p0[0] + ((p1[0] - p0[0]) * a + (p2[0] - p0[0]) * b) << " "
+        << p0[1] + ((p1[1] - p0[1]) * a + (p2[1] - p0[1]) * b) << std::endl;
+    }
+  }
+  if (!f.good()) return fail(nullptr, TSP_ERR_ARG, std::string("write failed: ") + fname);
+  return TSP_OK;
+}
+
+int tsp_eval_basis(int32_t N, int32_t basis, int32_t npts, const double* rpts, double* phi) {
+  if (N < 1 || N > tsp::kMaxN || npts < 0 || (npts > 0 && (!rpts || !phi)))
+    return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_eval_basis");
+  if (basis != TSP_BASIS_DUBINER && basis != TSP_BASIS_BOUNDARY_ADAPTED) return fail(nullptr, TSP_ERR_ARG, "bad basis");
+  const int Np = tsp::np_of(N);
+  for (int32_t q = 0; q < npts; ++q) tsp::basis_phi(basis, N, rpts[2 * q], rpts[2 * q + 1], phi + size_t(q) * Np);
+  return TSP_OK;
+}
+
+int tsp_quadrature_rule(int32_t N, double* rpts, double* w) {
+  if (N < 1 || N > tsp::kMaxN) return fail(nullptr, TSP_ERR_ARG, "degree N must be in 1..8");
+  std::vector<double> c, e, wq;
+  tsp::volume_rule(N, &c, &e, &wq);
+  for (size_t q = 0; q < wq.size(); ++q) {
+    if (rpts) {
+      rpts[2 * q] = c[q];
+      rpts[2 * q + 1] = e[q];
+    }
+    if (w) w[q] = wq[q];
+  }
+  return TSP_OK;
 }
 
 int tsp_get_ref_invmass(const tsp_handle* h, int32_t* basis, double* out) {

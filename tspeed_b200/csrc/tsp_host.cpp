@@ -503,7 +503,7 @@ bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int
   return true;
 }
 
-static void volume_rule(int N, std::vector<double>* c, std::vector<double>* e, std::vector<double>* w) {
+void volume_rule(int N, std::vector<double>* c, std::vector<double>* e, std::vector<double>* w) {
   const int Q = N + 1;
   std::vector<double> x(Q), wx(Q);
   gauleg(Q, -1.0, 1.0, x.data(), wx.data());

@@ -110,6 +110,13 @@ int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, co
 bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,
                std::vector<int32_t>* region, std::string* err);
 
+// The collapsed Gauss<N+1> volume rule on the reference triangle
+// (QuadratureRule_imp.hpp:101-113): (N+1)^2 nodes (c, e) and weights w.
+void volume_rule(int N, std::vector<double>* c, std::vector<double>* e, std::vector<double>* w);
+
+// Reference points of FESpace::field_out / points_out (FESpace_imp.hpp:31-34).
+constexpr double kFieldPoints[4][2] = {{0.2, 0.2}, {0.8, 0.2}, {0.2, 0.8}, {0.5, 0.5}};
+
 // Physical volume quadrature points of every element, [ne][Q*Q][2], in the
 // order of the collapsed Gauss<N+1> rule (QuadratureRule_imp.hpp:101-113)
 // mapped by Triangle::map (Geometry.cpp:203-207).

@@ -1780,4 +1780,47 @@ __global__ void __launch_bounds__(256) k_fold_basis(const double* in, int pin, i
   }
 }
 
+// The expansion of one shot's state at npt reference points of every
+// element: out[(e*npt + q)*2 + c] = sum_j T[q][j] u[(e*S + shot)*2Np + c*Np + j]
+// (T = basis values at the points, in the device's coordinates).
+__global__ void k_eval_points(const double* __restrict__ u, int ne, int S, int Np, int shot,
+                              const double* __restrict__ T, int npt, double* __restrict__ out) {
+  const long long n = 2ll * ne * npt;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const long long e = o / (2 * npt);
+    const int q = int((o / 2) % npt), c = int(o & 1);
+    const double* w = u + (e * S + shot) * 2 * Np + c * Np;
+    const double* t = T + size_t(q) * Np;
+    double v = 0.0;
+    for (int j = 0; j < Np; ++j) v = fma(t[j], w[j], v);
+    out[o] = v;
+  }
+}
+
+// Per-element terms of FESpace::L2error (FESpace_imp.hpp:107-133):
+// out[e] = detJ_e * sum_q w_q ((u_h,x(x_q) - ex_q,x)^2 + (u_h,y(x_q) - ex_q,y)^2),
+// points in order; the host adds the terms in element order.
+__global__ void k_l2_local(const double* __restrict__ u, int ne, int S, int Np, int shot,
+                           const double* __restrict__ T, const double* __restrict__ wq, int nq,
+                           const double* __restrict__ detJ, const double* __restrict__ exact,
+                           double* __restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const double* ux = u + ((long long)e * S + shot) * 2 * Np;
+    const double* uy = ux + Np;
+    const double* ex = exact + (long long)e * nq * 2;
+    double loc = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      const double* t = T + size_t(q) * Np;
+      double ax = 0.0, ay = 0.0;
+      for (int j = 0; j < Np; ++j) {
+        ax = fma(t[j], ux[j], ax);
+        ay = fma(t[j], uy[j], ay);
+      }
+      const double dx = ax - ex[2 * q], dy = ay - ex[2 * q + 1];
+      loc += (dx * dx + dy * dy) * wq[q];
+    }
+    out[e] = loc * detJ[e];
+  }
+}
+
 }  // namespace tsp
