@@ -332,6 +332,12 @@ int tsp_write_field(tsp_handle* h, int32_t shot, const char* fname, int64_t step
  * exact for |u_h|^2 but differ for a non-polynomial uex). Needs a handle
  * built from a mesh (TSP_ERR_UNSUPPORTED for tsp_create_from_blocks). */
 int tsp_l2_error(tsp_handle* h, int32_t shot, const double* exact, double* err);
+/* TimeAdvance::set_initial_u / set_initial_v (TimeAdvance_imp.hpp:42-51) with
+ * FESpace::transform on the device: field values at the volume quadrature
+ * points (tsp_quadrature_points order), [ne][(N+1)^2][2] each, projected
+ * into one shot's initial state (NULL: zero). Resets the step counter like
+ * tsp_set_initial. Needs a handle built from a mesh. */
+int tsp_set_initial_values(tsp_handle* h, int32_t shot, const double* u_vals, const double* v_vals);
 /* FESpace::points_out(fname): the physical positions of the field_out
  * points, one "x y" line per element and point. */
 int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const char* fname);

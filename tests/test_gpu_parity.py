@@ -565,3 +565,30 @@ def test_l2_error_needs_the_mesh():
             s.l2_error(np.zeros((g["tri"].shape[0], 9, 2)))
         assert e.value.code == -9
         assert s.field_values().shape == (g["tri"].shape[0], 4, 2)
+
+
+def test_golden_projection_on_the_device(golden):
+    """tsp_set_initial_values (FESpace::transform on the device) against the
+    reference's own transform of the generator's field, for u and v."""
+    g = golden
+    pts = capi.quadrature_points(int(g["N"]), g["xy"], g["tri"])
+    fx, fy = golden_field(g)(pts[..., 0], pts[..., 1])
+    vals = np.stack([fx, fy], -1)
+    with sim_from_golden(g) as s:
+        s.set_initial_values(0, vals, 2.0 * vals)
+        u0 = s.u()
+        _, _, k, _ = s.get_state()
+        s.first_step()
+        u1 = s.u()
+    tol = 1e-13 if basis_of(g) == "dubiner" else 1e-11  # cond(M_ref) for BoundaryAdapted
+    print(g["name"], "device projection", np.abs(u0 - g["proj"]).max() / np.abs(g["proj"]).max())
+    assert np.abs(u0 - g["proj"]).max() / np.abs(g["proj"]).max() < tol
+    assert k == 0
+    # LeapFrog::first_step from that state (u1 = u0 + dt v0 - dt^2/2 M^-1 (B u0 - f)).
+    o = oracle_setup(g)
+    ne, Np = g["tri"].shape[0], o["sp"].Np
+    proj = np.asarray(g["proj"])
+    ref1, _, _ = O.leapfrog(o["row_ptr"], o["cols"], o["blocks"], o["minv"], ne, Np, float(g["dt"]), 1,
+                            o["src_elem"], o["src_phi"], o["F"], o["rcv_elem"], o["rcv_phi"], u0=proj, v0=2.0 * proj,
+                            minv_ref=o["minv_ref"])
+    assert rel(u1, ref1) < tol

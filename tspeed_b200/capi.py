@@ -96,6 +96,7 @@ SIGNATURES = {
     "tsp_write_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int64]),
     "tsp_l2_error": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "tsp_points_out": (C.c_int, [C.c_int32, _dp, C.c_int32, _ip, C.c_char_p]),
+    "tsp_set_initial_values": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "tsp_eval_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
     "tsp_quadrature_rule": (C.c_int, [C.c_int32, _dp, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
@@ -292,6 +293,13 @@ class Simulation:
         u0 = None if u0 is None else _f64(u0)
         v0 = None if v0 is None else _f64(v0)
         _check(lib().tsp_set_initial(self._h, shot, _d(u0), _d(v0)), self._h)
+
+    def set_initial_values(self, shot: int, u_vals=None, v_vals=None):
+        """Initial u / v from field values at quadrature_points(), projected on
+        the device (FESpace::transform)."""
+        u_vals = None if u_vals is None else _f64(u_vals)
+        v_vals = None if v_vals is None else _f64(v_vals)
+        _check(lib().tsp_set_initial_values(self._h, shot, _d(u_vals), _d(v_vals)), self._h)
 
     def set_seismogram_capacity(self, n: int):
         _check(lib().tsp_set_seismogram_capacity(self._h, n), self._h)

@@ -1728,6 +1728,60 @@ int tsp_l2_error(tsp_handle* h, int32_t shot, const double* exact, double* err) 
   return check_device_error(h);
 }
 
+int tsp_set_initial_values(tsp_handle* h, int32_t shot, const double* u_vals, const double* v_vals) {
+  if (!h) return TSP_ERR_ARG;
+  if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
+  if (h->detJ.empty()) return fail(h, TSP_ERR_UNSUPPORTED, "the projection needs the mesh (handle built from blocks)");
+  int rc;
+  if ((rc = begin(h))) return rc;
+  const size_t nstate = size_t(h->ne) * h->S * h->R;
+  std::vector<double> c, e, w;
+  tsp::volume_rule(h->N, &c, &e, &w);
+  const int nq = int(w.size());
+  const std::vector<double> T = device_basis_table(h, nq, c.data(), e.data());
+  const size_t nv = size_t(h->ne) * nq * 2;
+  double *dT = nullptr, *dw = nullptr, *dJ = nullptr, *dval = nullptr;
+  auto cleanup = [&]() {
+    for (void* q : {(void*)dT, (void*)dw, (void*)dJ, (void*)dval}) dfree(h, q);
+  };
+  if ((rc = upload(h, &dT, T.data(), T.size())) || (rc = upload(h, &dw, w.data(), w.size())) ||
+      (rc = upload(h, &dJ, h->detJ.data(), h->detJ.size())) || (rc = dalloc(h, &dval, nv))) {
+    cleanup();
+    return rc;
+  }
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (v_vals && !h->d_v0) {
+    if ((rc = dalloc(h, &h->d_v0, nstate))) {
+      cleanup();
+      return rc;
+    }
+    TSP_CUDA(h, cudaMemsetAsync(h->d_v0, 0, nstate * sizeof(double), h->stream));
+  }
+  // Level u^0 lives in d_U[0] before first_step (as tsp_set_initial).
+  h->cur = 0;
+  cudaError_t ce = cudaSuccess;
+  for (int lvl = 0; lvl < 2 && ce == cudaSuccess; ++lvl) {
+    const double* vals = lvl == 0 ? u_vals : v_vals;
+    double* dst = lvl == 0 ? h->d_U[0] : h->d_v0;
+    if (!dst) continue;
+    if (vals) ce = cudaMemcpyAsync(dval, vals, nv * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (ce == cudaSuccess) {
+      tsp::k_project_points<<<1184, 256, 0, h->stream>>>(dst, h->ne, h->S, h->Np, shot, dT, dw, nq, dJ,
+                                                         vals ? dval : nullptr);
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+  }
+  cleanup();
+  if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("projection: ") + cudaGetErrorString(ce));
+  h->steps_done = 0;
+  h->last_time = 0.0;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+  clear_graphs(h);
+  return TSP_OK;
+}
+
 int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const char* fname) {
   if (nverts <= 0 || ne <= 0 || !xy || !tri || !fname) return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_points_out");
   for (int32_t i = 0; i < 3 * ne; ++i)

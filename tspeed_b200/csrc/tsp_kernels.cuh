@@ -1823,4 +1823,29 @@ __global__ void k_l2_local(const double* __restrict__ u, int ne, int S, int Np, 
   }
 }
 
+// FESpace::transform (FESpace_imp.hpp:136-179) on the device, written into
+// one shot's slot of a state buffer: for element e, component c and mode i,
+// u[(e*S + shot)*2Np + c*Np + i] = 1/detJ_e * sum_q T[q][i] f[e][q][c] |detJ_e| w_q,
+// with T the basis at the volume points in the device's coordinates
+// (L^-1 phi for a non-orthonormal basis, where w = L^T u = L^-1 rhs / detJ).
+// vals == nullptr writes zeros.
+__global__ void k_project_points(double* __restrict__ u, int ne, int S, int Np, int shot,
+                                 const double* __restrict__ T, const double* __restrict__ wq, int nq,
+                                 const double* __restrict__ detJ, const double* __restrict__ vals) {
+  const long long n = 2ll * ne * Np;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const long long e = o / (2 * Np);
+    const int r = int(o - e * 2 * Np), c = r >= Np ? 1 : 0, i = r - c * Np;
+    double v = 0.0;
+    if (vals) {
+      const double dJ = detJ[e], adJ = fabs(dJ);
+      const double* f = vals + e * nq * 2 + c;
+      double rhs = 0.0;
+      for (int q = 0; q < nq; ++q) rhs = fma(f[2 * q] * adJ * wq[q], T[size_t(q) * Np + i], rhs);
+      v = 1. / dJ * rhs;
+    }
+    u[(e * S + shot) * 2 * Np + r] = v;
+  }
+}
+
 }  // namespace tsp
