@@ -152,6 +152,13 @@ int tsp_create_from_blocks(const tsp_block_problem* prob, tsp_handle** out);
 /* Releases every resource of the handle. NULL is accepted. */
 int tsp_destroy(tsp_handle* h);
 
+/* Device memory of all handles comes from one stream-ordered pool per
+ * device that keeps freed memory cached for the process, so creating a
+ * simulation after destroying another does not pay for multi-GB device
+ * allocations again. This returns the cached memory of a device to the
+ * driver (after a device synchronisation). */
+int tsp_release_cached_memory(int32_t device);
+
 /* Message of the last failing call on this handle (or of the last failing
  * create, when h is NULL). Never NULL. */
 const char* tsp_last_error(const tsp_handle* h);
@@ -341,6 +348,12 @@ int tsp_set_initial_values(tsp_handle* h, int32_t shot, const double* u_vals, co
 /* FESpace::points_out(fname): the physical positions of the field_out
  * points, one "x y" line per element and point. */
 int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* tri, const char* fname);
+/* PointWiseEntity::M_add (Receivers_imp.hpp:34-51) for many points: the
+ * first (lowest-id) element passing Triangle::intriangle (Geometry.cpp:112-118)
+ * and the basis values at the point, elem[npts] (-1: outside the mesh),
+ * phi[npts][Np]. tsp_create locates sources and receivers with it. */
+int tsp_locate_points(int32_t N, int32_t basis, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri,
+                      int32_t npts, const double* pts, int32_t* elem, double* phi);
 /* Basis values at reference points (for callers holding u on the host):
  * rpts[npts][2] -> phi[npts][Np] (ShapeFunctions_imp.hpp). */
 int tsp_eval_basis(int32_t N, int32_t basis, int32_t npts, const double* rpts, double* phi);

@@ -165,3 +165,28 @@ def test_u_all_matches_per_shot_reads():
         allu = s.u_all()
         for k in range(len(shots)):
             assert np.array_equal(allu[k], s.u(k))
+
+
+def test_pooled_allocations_are_reused_and_released():
+    """Handles created one after the other draw on the library's cached
+    device pool; results do not depend on reuse, and the cache can be
+    returned to the driver."""
+    m = W.jittered_rect(6, 4, 600.0, 400.0, seed=81)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    rcv = W.surface_receivers(m, 3)
+    out = []
+    for _ in range(3):
+        with capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, [(300.0, 200.0)], rcv, penalty=10.0) as s:
+            s.set_dt(2e-4)
+            s.set_ricker(0, 25.0, 0.04, -1.0, 1, 60)
+            s.first_step()
+            s.run(59)
+            out.append(s.seismograms(0, 60))
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    capi.release_cached_memory(0)
+    with capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, [(300.0, 200.0)], rcv, penalty=10.0) as s:
+        s.set_dt(2e-4)
+        s.set_ricker(0, 25.0, 0.04, -1.0, 1, 60)
+        s.first_step()
+        s.run(59)
+        assert np.array_equal(s.seismograms(0, 60), out[0])

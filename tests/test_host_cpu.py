@@ -164,3 +164,34 @@ def test_eval_basis_and_quadrature_rule_match_oracle(N, basis):
     e = rng.random(30) * (1 - c)
     phi = capi.eval_basis(N, np.stack([c, e], -1), basis=basis)
     assert np.abs(phi - O.basis_phi(N, basis, c, e).T).max() < 1e-12
+
+
+@pytest.mark.parametrize("basis", ["dubiner", "ba"])
+def test_locate_points_matches_oracle_scan(basis):
+    """The grid-accelerated point location returns what the reference's
+    first-hit linear scan does (Receivers_imp.hpp:34-51): random interior
+    points, points on shared edges and vertices (the lowest id wins), and
+    points outside the mesh."""
+    N = 3
+    m = W.jittered_rect(12, 7, 1200.0, 700.0, seed=9)
+    rng = np.random.default_rng(3)
+    pts = [(1200 * rng.random(), 700 * rng.random()) for _ in range(200)]
+    pts += [tuple(m.xy[v]) for v in rng.integers(0, m.xy.shape[0], 40)]          # vertices
+    for e in rng.integers(0, m.ne, 40):                                           # edge midpoints
+        a, b = m.tri[e][0], m.tri[e][1]
+        pts.append(tuple(0.5 * (m.xy[a] + m.xy[b])))
+    pts += [(-5.0, 100.0), (600.0, 700.5), (1300.0, -20.0)]                       # outside
+    elem, phi = capi.locate_points(N, m.xy, m.tri, pts, basis=basis)
+    tri = m.tri.astype(np.int64)
+    geo = O.geometry(m.xy, tri)
+    for k, (x, y) in enumerate(pts):
+        try:
+            r = O.locate(N, m.xy, tri, geo, x, y, basis=basis)
+        except KeyError:
+            r = None
+        if r is None:
+            assert elem[k] == -1
+        else:
+            assert elem[k] == r[0]
+            ok = np.isfinite(r[1])
+            assert np.allclose(phi[k][ok], r[1][ok], rtol=0, atol=1e-12)

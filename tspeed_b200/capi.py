@@ -97,6 +97,8 @@ SIGNATURES = {
     "tsp_l2_error": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "tsp_points_out": (C.c_int, [C.c_int32, _dp, C.c_int32, _ip, C.c_char_p]),
     "tsp_set_initial_values": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
+    "tsp_release_cached_memory": (C.c_int, [C.c_int32]),
+    "tsp_locate_points": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int32, _ip, C.c_int32, _dp, _ip, _dp]),
     "tsp_eval_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
     "tsp_quadrature_rule": (C.c_int, [C.c_int32, _dp, _dp]),
     "tsp_gmsh_read": (C.c_int, [C.c_char_p, _ip, _dp, _ip, _ip, _ip]),
@@ -190,6 +192,17 @@ def points_out(xy, tri, fname: str):
     _check(lib().tsp_points_out(xy.shape[0], _d(xy), tri.shape[0], _i(tri), os.fsencode(fname)))
 
 
+def locate_points(N: int, xy, tri, pts, basis: str = "dubiner"):
+    """PointWiseEntity::M_add for many points: (elem[npts], phi[npts][Np])."""
+    xy, tri = _f64(xy), _i32(tri)
+    pts = _f64(np.asarray(pts, dtype=np.float64).reshape(-1, 2))
+    elem = np.zeros(pts.shape[0], dtype=np.int32)
+    phi = np.zeros((pts.shape[0], (N + 1) * (N + 2) // 2))
+    _check(lib().tsp_locate_points(N, TSP_BASIS[basis], xy.shape[0], _d(xy), tri.shape[0], _i(tri), pts.shape[0],
+                                   _d(pts), _i(elem), _d(phi)))
+    return elem, phi
+
+
 def eval_basis(N: int, rpts, basis: str = "dubiner"):
     """Basis values phi[npts][Np] at reference points rpts[npts][2]."""
     rpts = _f64(np.asarray(rpts, dtype=np.float64).reshape(-1, 2))
@@ -203,6 +216,11 @@ def quadrature_rule(N: int):
     r, w = np.zeros(((N + 1) ** 2, 2)), np.zeros((N + 1) ** 2)
     _check(lib().tsp_quadrature_rule(N, _d(r), _d(w)))
     return r, w
+
+
+def release_cached_memory(device: int = 0):
+    """Returns the device memory cached by the library's allocator pool."""
+    _check(lib().tsp_release_cached_memory(device))
 
 
 def force_times(dt: float, n: int):

@@ -125,23 +125,70 @@ int fail(tsp_handle* h, int code, const std::string& msg) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                             \
   } while (0)
 
+// Device memory of every handle comes from one stream-ordered pool per
+// device that keeps freed memory for the process (release threshold
+// unlimited): a program that creates and destroys simulations one after the
+// other (shot batches, parameter sweeps) pays cudaMalloc/cudaFree of the
+// multi-GB operator and state buffers once, not per simulation.
+// tsp_release_cached_memory returns the cached memory to the driver.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+cudaError_t device_pool(int dev, cudaMemPool_t* out) {
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mutex);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~uint64_t(0);
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return cudaSuccess;
+}
+
+// Allocation on the handle's stream, completed before returning so that the
+// memory may be used from any stream or by synchronous copies.
+cudaError_t pool_alloc(tsp_handle* h, void** p, size_t bytes) {
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = device_pool(h->device, &pool);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e;
+}
+
 template <typename T>
 int dalloc(tsp_handle* h, T** p, size_t n) {
   *p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  void* q = nullptr;
+  cudaError_t e = pool_alloc(h, &q, n * sizeof(T));
   if (e != cudaSuccess)
-    return fail(h, TSP_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) + " bytes: " +
+    return fail(h, TSP_ERR_NOMEM, std::string("device allocation of ") + std::to_string(n * sizeof(T)) + " bytes: " +
                                       cudaGetErrorString(e));
-  h->owned.push_back(*p);
+  *p = static_cast<T*>(q);
+  h->owned.push_back(q);
   return TSP_OK;
 }
 
+// Stream-ordered release: work already queued on the handle's stream that
+// reads p completes first.
 void dfree(tsp_handle* h, void* p) {
   if (!p) return;
   auto it = std::find(h->owned.begin(), h->owned.end(), p);
   if (it != h->owned.end()) h->owned.erase(it);
-  cudaFree(p);
+  cudaFreeAsync(p, h->stream);
 }
 
 template <typename T>
@@ -792,6 +839,8 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
     return fail(nullptr, TSP_ERR_UNSUPPORTED, "the matrix-free operator is built for the orthonormal Dubiner basis");
   for (int32_t i = 0; i < 3 * P->ne; ++i)
     if (P->tri[i] < 0 || P->tri[i] >= P->nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  for (int32_t i = 0; i < 2 * P->nverts; ++i)
+    if (!std::isfinite(P->xy[i])) return fail(nullptr, TSP_ERR_MESH, "vertex coordinates must be finite");
   for (int32_t e = 0; e < P->ne; ++e)
     if (!(P->rho[e] > 0) || !(P->mu[e] >= 0) || !std::isfinite(P->lambda[e]))
       return fail(nullptr, TSP_ERR_ARG, "material values must be finite with rho > 0, mu >= 0");
@@ -832,28 +881,25 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   tsp::RefTables T = tsp::make_tables(P->N, P->basis);
   if (P->basis != TSP_BASIS_DUBINER && (rc = set_basis_mass(h, P->basis, T.M, T.Minv))) return create_error_from(h, rc);
 
-  // ---- sources and receivers ----
-  h->src_elem.resize(h->S);
-  h->src_phi.resize(size_t(h->S) * h->Np);
-  for (int s = 0; s < h->S; ++s) {
-    const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->src_xy[2 * s], P->src_xy[2 * s + 1],
-                                    &h->src_phi[size_t(s) * h->Np], P->basis);
-    if (e < 0) {
-      fail(h, TSP_ERR_NOT_FOUND, "source point " + std::to_string(s) + " not found in the mesh");
-      return create_error_from(h, TSP_ERR_NOT_FOUND);
-    }
-    h->src_elem[s] = e;
-  }
-  h->rcv_elem.resize(h->nrcv);
-  h->rcv_phi.resize(size_t(h->nrcv) * h->Np);
-  for (int r = 0; r < h->nrcv; ++r) {
-    const int e = tsp::locate_point(P->N, P->ne, P->xy, P->tri, g, P->rcv_xy[2 * r], P->rcv_xy[2 * r + 1],
-                                    &h->rcv_phi[size_t(r) * h->Np], P->basis);
-    if (e < 0) {
-      fail(h, TSP_ERR_NOT_FOUND, "receiver point " + std::to_string(r) + " not found in the mesh");
-      return create_error_from(h, TSP_ERR_NOT_FOUND);
-    }
-    h->rcv_elem[r] = e;
+  // ---- sources and receivers (one point-location pass for both) ----
+  {
+    const int np_all = h->S + h->nrcv;
+    std::vector<double> pts(2 * size_t(np_all)), phi(size_t(np_all) * h->Np);
+    std::vector<int32_t> el(np_all);
+    std::copy(P->src_xy, P->src_xy + 2 * size_t(h->S), pts.begin());
+    if (h->nrcv) std::copy(P->rcv_xy, P->rcv_xy + 2 * size_t(h->nrcv), pts.begin() + 2 * size_t(h->S));
+    tsp::locate_points(P->N, P->ne, P->xy, P->tri, g, np_all, pts.data(), el.data(), phi.data(), P->basis);
+    for (int k = 0; k < np_all; ++k)
+      if (el[k] < 0) {
+        const bool src = k < h->S;
+        fail(h, TSP_ERR_NOT_FOUND, std::string(src ? "source" : "receiver") + " point " +
+                                       std::to_string(src ? k : k - h->S) + " not found in the mesh");
+        return create_error_from(h, TSP_ERR_NOT_FOUND);
+      }
+    h->src_elem.assign(el.begin(), el.begin() + h->S);
+    h->rcv_elem.assign(el.begin() + h->S, el.end());
+    h->src_phi.assign(phi.begin(), phi.begin() + size_t(h->S) * h->Np);
+    h->rcv_phi.assign(phi.begin() + size_t(h->S) * h->Np, phi.end());
   }
 
   // ---- device upload + assembly ----
@@ -922,7 +968,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
   const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
   {
     void* blk = nullptr;
-    cudaError_t ce = cudaMalloc(&blk, size_t(h->nnzb) * RRp * esz);
+    cudaError_t ce = pool_alloc(h, &blk, size_t(h->nnzb) * RRp * esz);
     if (ce != cudaSuccess) {
       fail(h, TSP_ERR_NOMEM, "operator blocks (" + std::to_string(size_t(h->nnzb) * RRp * esz) +
                                  " bytes) do not fit: " + cudaGetErrorString(ce));
@@ -1107,9 +1153,30 @@ int tsp_destroy(tsp_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   clear_graphs(h);
-  for (void* p : h->owned) cudaFree(p);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  for (void* p : h->owned) cudaFreeAsync(p, h->stream);
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
   delete h;
+  return TSP_OK;
+}
+
+int tsp_release_cached_memory(int32_t device) {
+  if (device < 0 || device >= kMaxDevices) return fail(nullptr, TSP_ERR_ARG, "device ordinal out of range");
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mutex);
+    pool = g_pools[device];
+  }
+  if (!pool) return TSP_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(nullptr, TSP_ERR_CUDA, std::string("pool trim: ") + cudaGetErrorString(e));
   return TSP_OK;
 }
 
@@ -1800,6 +1867,21 @@ int tsp_points_out(int32_t nverts, const double* xy, int32_t ne, const int32_t* 
     }
   }
   if (!f.good()) return fail(nullptr, TSP_ERR_ARG, std::string("write failed: ") + fname);
+  return TSP_OK;
+}
+
+int tsp_locate_points(int32_t N, int32_t basis, int32_t nverts, const double* xy, int32_t ne, const int32_t* tri,
+                      int32_t npts, const double* pts, int32_t* elem, double* phi) {
+  if (N < 1 || N > tsp::kMaxN || nverts <= 0 || ne <= 0 || !xy || !tri || npts < 0 ||
+      (npts > 0 && (!pts || !elem || !phi)))
+    return fail(nullptr, TSP_ERR_ARG, "bad arguments to tsp_locate_points");
+  if (basis != TSP_BASIS_DUBINER && basis != TSP_BASIS_BOUNDARY_ADAPTED) return fail(nullptr, TSP_ERR_ARG, "bad basis");
+  for (int32_t i = 0; i < 3 * ne; ++i)
+    if (tri[i] < 0 || tri[i] >= nverts) return fail(nullptr, TSP_ERR_MESH, "vertex id out of range");
+  for (int32_t i = 0; i < 2 * nverts; ++i)
+    if (!std::isfinite(xy[i])) return fail(nullptr, TSP_ERR_MESH, "vertex coordinates must be finite");
+  const tsp::Geometry g = tsp::make_geometry(ne, xy, tri);
+  tsp::locate_points(N, ne, xy, tri, g, npts, pts, elem, phi, basis);
   return TSP_OK;
 }
 

@@ -398,31 +398,111 @@ void bsr_pattern(int32_t ne, const int32_t* neigh, std::vector<int32_t>* row_ptr
   }
 }
 
+namespace {
+
+// Padded bounding box of element e. The pad covers every point the
+// containment test below accepts: its tolerances are absolute in units of
+// twice the area, i.e. a distance of about 1e-6 / (edge length) outside an
+// edge, which the 1e-4 / (w + h) term bounds for any element size.
+void element_box(const double* xy, const int32_t* tri, int32_t e, double box[4]) {
+  const double* p0 = xy + 2 * size_t(tri[3 * size_t(e)]);
+  const double* p1 = xy + 2 * size_t(tri[3 * size_t(e) + 1]);
+  const double* p2 = xy + 2 * size_t(tri[3 * size_t(e) + 2]);
+  const double xmin = std::fmin(p0[0], std::fmin(p1[0], p2[0])), xmax = std::fmax(p0[0], std::fmax(p1[0], p2[0]));
+  const double ymin = std::fmin(p0[1], std::fmin(p1[1], p2[1])), ymax = std::fmax(p0[1], std::fmax(p1[1], p2[1]));
+  const double wh = (xmax - xmin) + (ymax - ymin);
+  const double pad = 1e-3 * wh + 1e-6 + (wh > 0 ? 1e-4 / wh : 0.0);
+  box[0] = xmin - pad;
+  box[1] = xmax + pad;
+  box[2] = ymin - pad;
+  box[3] = ymax + pad;
+}
+
+// Triangle::intriangle (Geometry.cpp:112-118) and invmap (Geometry.cpp:199-202)
+// of element e; on success the basis values at the point go to phi.
+bool try_element(int N, int basis, const double* xy, const int32_t* tri, const Geometry& g, int32_t e, double px,
+                 double py, double* phi) {
+  double box[4];
+  element_box(xy, tri, e, box);
+  if (px < box[0] || px > box[1] || py < box[2] || py > box[3]) return false;
+  const double* p0 = xy + 2 * size_t(tri[3 * size_t(e)]);
+  const double* p1 = xy + 2 * size_t(tri[3 * size_t(e) + 1]);
+  const double* p2 = xy + 2 * size_t(tri[3 * size_t(e) + 2]);
+  const double s = p0[1] * p2[0] - p0[0] * p2[1] + (p2[1] - p0[1]) * px + (p0[0] - p2[0]) * py;
+  const double t = p0[0] * p1[1] - p0[1] * p1[0] + (p0[1] - p1[1]) * px + (p1[0] - p0[0]) * py;
+  const double A = 1. / 2. * (-p1[1] * p2[0] + p0[1] * (-p1[0] + p2[0]) + p0[0] * (p1[1] - p2[1]) + p1[0] * p2[1]);
+  if (!(s > -1e-6 && t > -1e-6 && (s + t) < (2 + 1e-6) * A)) return false;
+  const double* iJ = &g.invJ[4 * size_t(e)];
+  const double dx = px - p0[0], dy = py - p0[1];
+  const double r0 = iJ[0] * dx + iJ[2] * dy;
+  const double r1 = iJ[1] * dx + iJ[3] * dy;
+  basis_phi(basis, N, r0, r1, phi);
+  return true;
+}
+
+}  // namespace
+
 int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, double px,
                      double py, double* phi, int basis) {
-  for (int32_t e = 0; e < ne; ++e) {
-    const double* p0 = xy + 2 * size_t(tri[3 * size_t(e)]);
-    const double* p1 = xy + 2 * size_t(tri[3 * size_t(e) + 1]);
-    const double* p2 = xy + 2 * size_t(tri[3 * size_t(e) + 2]);
-    // Cheap rejection: the tolerance below is absolute and tiny, so a point
-    // far outside the bounding box can never pass.
-    const double xmin = std::fmin(p0[0], std::fmin(p1[0], p2[0])), xmax = std::fmax(p0[0], std::fmax(p1[0], p2[0]));
-    const double ymin = std::fmin(p0[1], std::fmin(p1[1], p2[1])), ymax = std::fmax(p0[1], std::fmax(p1[1], p2[1]));
-    const double pad = 1e-3 * ((xmax - xmin) + (ymax - ymin)) + 1e-6;
-    if (px < xmin - pad || px > xmax + pad || py < ymin - pad || py > ymax + pad) continue;
-    const double s = p0[1] * p2[0] - p0[0] * p2[1] + (p2[1] - p0[1]) * px + (p0[0] - p2[0]) * py;
-    const double t = p0[0] * p1[1] - p0[1] * p1[0] + (p0[1] - p1[1]) * px + (p1[0] - p0[0]) * py;
-    const double A = 1. / 2. * (-p1[1] * p2[0] + p0[1] * (-p1[0] + p2[0]) + p0[0] * (p1[1] - p2[1]) + p1[0] * p2[1]);
-    if (s > -1e-6 && t > -1e-6 && (s + t) < (2 + 1e-6) * A) {
-      const double* iJ = &g.invJ[4 * size_t(e)];
-      const double dx = px - p0[0], dy = py - p0[1];
-      const double r0 = iJ[0] * dx + iJ[2] * dy;
-      const double r1 = iJ[1] * dx + iJ[3] * dy;
-      basis_phi(basis, N, r0, r1, phi);
-      return e;
-    }
-  }
+  for (int32_t e = 0; e < ne; ++e)
+    if (try_element(N, basis, xy, tri, g, e, px, py, phi)) return e;
   return -1;
+}
+
+void locate_points(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, int32_t npts,
+                   const double* pts, int32_t* elem, double* phi, int basis) {
+  const int Np = np_of(N);
+  if (npts <= 4) {
+    for (int32_t k = 0; k < npts; ++k)
+      elem[k] = locate_point(N, ne, xy, tri, g, pts[2 * k], pts[2 * k + 1], phi + size_t(k) * Np, basis);
+    return;
+  }
+  // Uniform grid over the padded boxes, about one element per cell; each
+  // cell lists, in increasing id, every element whose padded box meets it.
+  std::vector<double> boxes(size_t(ne) * 4);
+  double X0 = 1e300, X1 = -1e300, Y0 = 1e300, Y1 = -1e300;
+  for (int32_t e = 0; e < ne; ++e) {
+    double* b = &boxes[size_t(e) * 4];
+    element_box(xy, tri, e, b);
+    X0 = std::fmin(X0, b[0]);
+    X1 = std::fmax(X1, b[1]);
+    Y0 = std::fmin(Y0, b[2]);
+    Y1 = std::fmax(Y1, b[3]);
+  }
+  const double W = std::fmax(X1 - X0, 1e-300), H = std::fmax(Y1 - Y0, 1e-300);
+  const double cells = std::fmax(1.0, double(ne));
+  int nx = int(std::ceil(std::sqrt(cells * W / H)));
+  int ny = int(std::ceil(cells / nx));
+  nx = std::max(1, std::min(nx, 1 << 14));
+  ny = std::max(1, std::min(ny, 1 << 14));
+  auto cx = [&](double x) { return std::min(nx - 1, std::max(0, int((x - X0) / W * nx))); };
+  auto cy = [&](double y) { return std::min(ny - 1, std::max(0, int((y - Y0) / H * ny))); };
+  const size_t ncell = size_t(nx) * ny;
+  std::vector<int64_t> start(ncell + 1, 0);
+  for (int32_t e = 0; e < ne; ++e) {
+    const double* b = &boxes[size_t(e) * 4];
+    for (int iy = cy(b[2]); iy <= cy(b[3]); ++iy)
+      for (int ix = cx(b[0]); ix <= cx(b[1]); ++ix) start[size_t(iy) * nx + ix + 1]++;
+  }
+  for (size_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+  std::vector<int32_t> list(size_t(start[ncell]));
+  std::vector<int64_t> fill(start.begin(), start.end() - 1);
+  for (int32_t e = 0; e < ne; ++e) {
+    const double* b = &boxes[size_t(e) * 4];
+    for (int iy = cy(b[2]); iy <= cy(b[3]); ++iy)
+      for (int ix = cx(b[0]); ix <= cx(b[1]); ++ix) list[size_t(fill[size_t(iy) * nx + ix]++)] = e;
+  }
+  for (int32_t k = 0; k < npts; ++k) {
+    const double px = pts[2 * k], py = pts[2 * k + 1];
+    elem[k] = -1;
+    if (!(px >= X0 && px <= X1 && py >= Y0 && py <= Y1)) continue;  // outside every padded box (or NaN)
+    const size_t c = size_t(cy(py)) * nx + cx(px);
+    for (int64_t i = start[c]; i < start[c + 1]; ++i)
+      if (try_element(N, basis, xy, tri, g, list[size_t(i)], px, py, phi + size_t(k) * Np)) {
+        elem[k] = list[size_t(i)];
+        break;
+      }
+  }
 }
 
 bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,

@@ -106,6 +106,13 @@ void bsr_pattern(int32_t ne, const int32_t* neigh, std::vector<int32_t>* row_ptr
 int32_t locate_point(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, double px,
                      double py, double* phi, int basis = kDubiner);
 
+// locate_point for many points with the same result: a uniform grid over the
+// elements' padded bounding boxes gives each point its candidate elements in
+// increasing id, and the first one passing the same test is taken.
+// elem[k] = -1 where none does.
+void locate_points(int N, int32_t ne, const double* xy, const int32_t* tri, const Geometry& g, int32_t npts,
+                   const double* pts, int32_t* elem, double* phi, int basis = kDubiner);
+
 // Gmsh 2.2 ASCII reader (Mesh.cpp:174-257).
 bool gmsh_read(const std::string& path, std::vector<double>* xy, std::vector<int32_t>* tri,
                std::vector<int32_t>* region, std::string* err);
