@@ -592,3 +592,41 @@ def test_golden_projection_on_the_device(golden):
                             o["src_elem"], o["src_phi"], o["F"], o["rcv_elem"], o["rcv_phi"], u0=proj, v0=2.0 * proj,
                             minv_ref=o["minv_ref"])
     assert rel(u1, ref1) < tol
+
+
+@pytest.mark.parametrize("N", [1, 3, 5, 6])
+def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
+    """FP64 with several shots runs on the FP64 tensor cores (DMMA): the
+    warp-specialised persistent kernel (default) and the single-role one
+    (TSP_BATCHED_VARIANT=3); the register-staged CUDA-core kernel (=2)
+    computes the same products in another order: all agree to rounding, over
+    full and partial shot tiles, with the energy monitor on."""
+    m = W.jittered_rect(6, 5, 600.0, 500.0, seed=90 + N)
+    rng = np.random.default_rng(N)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    shots = [(30 + 540 * rng.random(), 30 + 440 * rng.random()) for _ in range(70)]
+    rcv = W.surface_receivers(m, 4)
+    n = 80
+    out = {}
+    dt = None
+    for variant in ("auto", "3", "2"):
+        if variant != "auto":
+            monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+        else:
+            monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0) as s:
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
+            s.set_dt(dt)
+            for k in range(len(shots)):
+                s.set_ricker(k, 25.0, 0.04, -1.0, k % 2, n)
+            s.set_seismogram_capacity(n)
+            s.enable_energy(True)
+            s.first_step()
+            s.run(n - 1)
+            out[variant] = (s.seismograms(0, n), s.u_all(), s.energy(1, n - 1))
+    for v in ("auto", "3"):
+        for i in range(3):
+            print("N", N, v, i, rel(out[v][i], out["2"][i]))
+            assert rel(out[v][i], out["2"][i]) < 1e-13

@@ -20,6 +20,7 @@
 #include "tsp_kernels.cuh"
 #include "tsp_tcgen05.cuh"
 #include "tsp_tcfx.cuh"
+#include "tsp_dmma.cuh"
 
 namespace {
 
@@ -469,6 +470,43 @@ int launch_batched(tsp_handle* h, const tsp::StepParams& p, dim3 grid, cudaStrea
   return TSP_OK;
 }
 
+template <int R>
+int launch_d64(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  typedef tsp::D64Cfg<R> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;  // one bit per device
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched64d<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP64 batched kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
+  tsp::k_step_batched64d<R><<<grid, CF::NT, smem, st>>>(p);
+  return TSP_OK;
+}
+
+template <int R>
+int launch_d64w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  constexpr int NST = 5;
+  typedef tsp::D64WCfg<R, NST> CF;
+  const size_t smem = CF::smem_bytes();
+  static unsigned long long configured = 0;  // one bit per device
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e =
+        cudaFuncSetAttribute(tsp::k_step_batched64w<R, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP64 batched kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  // Persistent: one CTA per SM.
+  const long long items = (long long)h->ne * ((h->S + CF::ST - 1) / CF::ST);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched64w<R, NST><<<grid, CF::NT, smem, st>>>(p, h->d_err);
+  return TSP_OK;
+}
+
 template <int N>
 int launch_matfree_N(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::MFCfg<N> CF;
@@ -586,6 +624,14 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
     const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
     tsp::k_step_batched32<R><<<grid, CF::NT, smem, st>>>(p);
     return TSP_OK;
+  }
+  // FP64 with several shots: the FP64 tensor-core (DMMA) kernels, the
+  // warp-specialised persistent one by default; TSP_BATCHED_VARIANT=3 selects
+  // the single-role DMMA kernel and 2 the register-staged CUDA-core kernel.
+  if constexpr (R <= 56) {
+    if (h->S > 1 && h->prec == TSP_PREC_FP64 && h->kernel_variant != 2 &&
+        (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
+      return h->kernel_variant == 3 ? launch_d64<R>(h, p, st) : launch_d64w<R>(h, p, st);
   }
   if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::BatchCfg<R> CF;

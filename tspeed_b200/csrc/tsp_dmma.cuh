@@ -1,0 +1,246 @@
+// Batched FP64 step on the FP64 tensor cores, warp-specialised and
+// persistent (internal header of tspeed_b200).
+//
+// The same product as k_step_batched64d -- per work item (element row e,
+// tile of ST shots) Y[shot][r] = sum_b sum_k X_{col b}[shot][k] B_b[r][k]
+// with mma.sync m8n8k4 .f64 (exact FP64 products, FP64 accumulation) -- but
+// the operands stream through an NST-stage ring in shared memory filled by a
+// producer warp with bulk copies (cp.async.bulk, completion on mbarriers, no
+// multicast), so the consumer warps never wait on their own copies and the
+// next item's blocks arrive while the current item's epilogue runs.
+//
+// Roles: warps 0..NCW-1 consume (WM x WN warps, each MTW m-tiles of 8
+// shots x NTW n-tiles of 8 operator rows; accumulators in registers; they
+// also run the leap-frog epilogue, receivers and energy); warp NCW produces.
+// Per block the producer issues two bulk copies: the operator block as it is
+// stored (column-major, pitch KP = R padded to 4, padding rows zero) and the
+// state tile of the neighbour (ST shot rows of R doubles, contiguous in the
+// state layout). Many small copies would be limited by the copy engine's
+// request rate; two large ones are not. The K padding of the operator
+// (columns R..KP-1) is zeroed once and never written, so the state's K
+// padding (the next shot row's first entries, or zeroed slack) multiplies
+// zeros; outputs of padded rows and of shots beyond S are discarded. The
+// stages are zeroed once so that no entry ever read is uninitialised.
+//
+// Every wait is bounded (about a second); on a timeout the CTA raises an
+// abort flag in shared memory, every role stops waiting, the consumer warps
+// keep their named barriers balanced, the producer waits (bounded) for its
+// copies in flight, and err_flag tells the host that the results are void.
+#pragma once
+
+#include <stdint.h>
+
+#include "tsp_kernels.cuh"
+#include "tsp_tcfx.cuh"
+#include "tsp_tcgen05.cuh"
+
+namespace tsp {
+
+template <int R, int NST_>
+struct D64WCfg {
+  static constexpr int KP = (R + 3) & ~3;  // also the stored block pitch of batched handles
+  static constexpr int NTL = (R + 7) / 8;
+  static constexpr int ST = R <= 42 ? 64 : 32;
+  static constexpr int WM = 4, WN = 2, NCW = WM * WN;
+  static constexpr int MTW = ST / (8 * WM);
+  static constexpr int NTW = (NTL + WN - 1) / WN;
+  static constexpr int NT = (NCW + 1) * 32;
+  static constexpr int NST = NST_;
+  static constexpr int BSZ = KP * KP;      // doubles: operator stage [k][n], pitch KP
+  static constexpr int XSZ = ST * R + 4;   // doubles: state stage [shot][k], pitch R, zero slack
+  static constexpr int STAGE = BSZ + XSZ;
+  static constexpr size_t smem_bytes() {
+    return size_t(NST) * STAGE * sizeof(double) + size_t(2 * NST) * sizeof(uint64_t) + 16;
+  }
+};
+
+template <int R, int NST>
+__global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(const StepParams p, int* err_flag) {
+  typedef D64WCfg<R, NST> CF;
+  constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* stages = reinterpret_cast<double*>(smem_raw);
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NST] stage landed
+  uint64_t* bempty = bfull + NST;                                                    // [NST] stage consumed
+  volatile int* abort_s = reinterpret_cast<volatile int*>(bempty + NST);
+
+  if (*reinterpret_cast<volatile int*>(err_flag) != 0) return;  // an earlier launch of the run timed out
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (t == 0) {
+    *abort_s = 0;
+    for (int i = 0; i < NST; ++i) {
+      fx_mbar_init(smem_u32(&bfull[i]), 1);
+      fx_mbar_init(smem_u32(&bempty[i]), CF::NCW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = t; i < NST * CF::STAGE; i += CF::NT) stages[i] = 0.0;
+  __syncthreads();
+
+  const int S = p.S;
+  const int ntile = (S + ST - 1) / ST;
+  const long long nitems = (long long)p.ne * ntile;
+  const long long G = gridDim.x;
+  const double* blocks = reinterpret_cast<const double*>(p.blocks);
+
+  if (warp == CF::NCW) {
+    // ---------------- producer ----------------
+    uint32_t j = 0;
+    bool ok = true;
+    for (long long item = blockIdx.x; item < nitems && ok; item += G) {
+      const int e = int(item / ntile), tile = int(item % ntile);
+      const int s0 = tile * ST, nsh = min(ST, S - s0);
+      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      const uint32_t bbytes = uint32_t(R) * KP * 8, xbytes = uint32_t(nsh) * R * 8;
+      for (int b = 0; b < nb; ++b) {
+        const int s = int(j % NST);
+        const uint32_t n = j / NST;
+        int okl = 1;
+        if (lane == 0 && n > 0) okl = fx_wait(smem_u32(&bempty[s]), (n - 1) & 1, abort_s) ? 1 : 0;
+        if (!__shfl_sync(0xffffffffu, okl, 0)) {
+          ok = false;
+          break;
+        }
+        if (lane == 0) {
+          const int c = p.col[rb + b];
+          const uint32_t bar = smem_u32(&bfull[s]);
+          const uint32_t dB = smem_u32(stages + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 8;
+          fx_mbar_arrive_tx(bar, bbytes + xbytes);
+          fx_bulk_g2s(dB, blocks + size_t(rb + b) * R * KP, bbytes, bar);
+          fx_bulk_g2s(dX, p.x + (size_t(c) * S + s0) * R, xbytes, bar);
+        }
+        ++j;
+      }
+    }
+    // Every issued copy lands before the CTA ends (bounded; copies complete).
+    if (lane == 0) {
+      const long long t0 = clock64();
+      for (int s = 0; s < NST; ++s) {
+        if (j <= uint32_t(s)) continue;
+        const uint32_t uses = (j - 1 - s) / NST + 1;
+        while (!mbar_try(smem_u32(&bfull[s]), (uses - 1) & 1) && clock64() - t0 < (1ll << 31)) {
+        }
+      }
+      if (clock64() - t0 >= (1ll << 31)) *abort_s = 1;
+    }
+  } else {
+    // ---------------- consumers ----------------
+    const int wm = warp % CF::WM, wn = warp / CF::WM;
+    const int g = lane >> 2, tg = lane & 3;
+    const int nt0 = wn * NTW, ntn = min(NTW, NTL - nt0);
+    const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+    const double dt = p.dt;
+    double en = 0.0;
+    uint32_t j = 0;
+    bool dead = false;
+    for (long long item = blockIdx.x; item < nitems; item += G) {
+      const int e = int(item / ntile), tile = int(item % ntile);
+      const int s0 = tile * ST;
+      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      double acc[MTW][NTW][2];
+#pragma unroll
+      for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) acc[mt][q][0] = acc[mt][q][1] = 0.0;
+      for (int b = 0; b < nb; ++b) {
+        const int s = int(j % NST);
+        const uint32_t n = j / NST;
+        ++j;
+        if (dead) continue;
+        const bool okw = fx_wait(smem_u32(&bfull[s]), n & 1, abort_s);
+        if (__any_sync(0xffffffffu, !okw)) {
+          dead = true;
+          continue;
+        }
+        const double* B = stages + size_t(s) * CF::STAGE;
+        const double* X = B + CF::BSZ + (wm * MTW * 8 + g) * R + tg;
+        const double* Bt = B + tg * KP + nt0 * 8 + g;
+#pragma unroll
+        for (int k0 = 0; k0 < KP; k0 += 4) {
+          double a[MTW], bb[NTW];
+#pragma unroll
+          for (int mt = 0; mt < MTW; ++mt) a[mt] = X[mt * 8 * R + k0];
+#pragma unroll
+          for (int q = 0; q < NTW; ++q) bb[q] = (NTL % CF::WN == 0 || q < ntn) ? Bt[k0 * KP + q * 8] : 0.0;
+#pragma unroll
+          for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+            for (int q = 0; q < NTW; ++q)
+              if (NTL % CF::WN == 0 || q < ntn) dmma_m8n8k4(acc[mt][q][0], acc[mt][q][1], a[mt], bb[q]);
+        }
+        __syncwarp();
+        if (lane == 0) fx_mbar_arrive(smem_u32(&bempty[s]));
+      }
+      // ---- epilogue (leap-frog, source, energy terms) ----
+      if (!dead) {
+        const double mi = p.minv[e];
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt) {
+          const int sh = s0 + (wm * MTW + mt) * 8 + g;
+          if (sh >= S) continue;
+          const size_t me = (size_t(e) * S + sh) * R;
+          const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+          double Fk[2] = {0.0, 0.0};
+          if (is_src) {
+            Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+            Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+          }
+#pragma unroll
+          for (int q = 0; q < NTW; ++q) {
+            const int r0 = (nt0 + q) * 8 + 2 * tg;
+            if (q >= ntn || r0 >= R) continue;  // rows come in pairs (R is even)
+            const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
+            const double2 up =
+                p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
+            const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+            double un[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r = r0 + h;
+              const int cmp = r / NP, ii = r - cmp * NP;
+              const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+              const double y = acc[mt][q][h];
+              if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+              else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+              if (p.energy != nullptr) {
+                const double d = un[h] - u[h];
+                en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+              }
+            }
+            *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+          }
+        }
+      }
+      // ---- receivers (the condition is the same for every consumer warp) ----
+      if (p.rcv_ptr != nullptr) {
+        const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+        if (q1 > q0) {
+          fx_epi_sync<CF::NCW * 32>();  // u^{k+1} of this item is visible to all consumers
+          if (!dead) {
+            const long long slot = k % p.seis_cap;
+            const int nwork = (q1 - q0) * ST * 2;
+            for (int wk = t; wk < nwork; wk += CF::NCW * 32) {
+              const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
+              const int sh = s0 + sl;
+              if (sh >= S) continue;
+              const int rid = p.rcv_id[q];
+              const double* ph = p.rcv_phi + size_t(rid) * NP;
+              const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+              double v = 0.0;
+              for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+              p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+            }
+          }
+        }
+      }
+    }
+    if (p.energy != nullptr) {
+      const double v = warp_sum(en);
+      if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
+    }
+  }
+  __syncthreads();
+  if (t == 0 && *abort_s) atomicExch(err_flag, 1);
+}
+
+}  // namespace tsp

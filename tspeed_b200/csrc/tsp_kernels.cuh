@@ -562,6 +562,218 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
 }
 
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Batched FP64 step on the FP64 tensor cores (DMMA, mma.sync m8n8k4 .f64).
+// Exact FP64 products and FP64 accumulation, so the result is the plain
+// FP64 step's up to summation order. Per CTA: one element row and a tile of
+// ST shots; per block of the row, Y[shot][r] += X_c[shot][k] B[r][k] as a
+// (ST x KP) . (KP x 8*NTL) product, KP = R padded to the MMA's k = 4.
+// The WM x WN warps split it: warp (wm, wn) owns MTW m-tiles of 8 shots
+// and NTW n-tiles of 8 operator rows. Blocks and the neighbours' state tiles
+// are staged global->shared with 16-byte cp.async into a two-stage ring
+// (block b+1 copies while block b multiplies). Shared pitches PS satisfy
+// PS mod 16 in {4, 12}, which makes both fragment loads conflict-free.
+// The K padding (columns R..KP-1 of X and of B) is zeroed once; C columns
+// n >= R read operator entries of the next column and are discarded.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int d64_pitch(int kp) { return (kp % 16 == 4 || kp % 16 == 12) ? kp : d64_pitch(kp + 2); }
+
+template <int R>
+struct D64Cfg {
+  static constexpr int KP = (R + 3) & ~3;
+  static constexpr int NTL = (R + 7) / 8;
+  static constexpr int PS = d64_pitch(KP);
+  static constexpr int ST = R <= 42 ? 64 : 32;     // shots per CTA
+  static constexpr int WM = 4, WN = 2, WARPS = WM * WN;
+  static constexpr int MTW = ST / (8 * WM);        // m-tiles per warp
+  static constexpr int NTW = (NTL + WN - 1) / WN;  // n-tiles per warp
+  static constexpr int NT = WARPS * 32;
+  static constexpr int BSZ = KP * PS;              // doubles: B stage [k][n]
+  static constexpr int XSZ = ST * PS;              // doubles: X stage [shot][k]
+  static constexpr int STAGE = BSZ + XSZ;
+  static constexpr size_t smem_bytes() { return size_t(2) * STAGE * sizeof(double) + WARPS * sizeof(double); }
+};
+
+__device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int R>
+__global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const StepParams p) {
+  typedef D64Cfg<R> CF;
+  constexpr int NP = R / 2, KP = CF::KP, PS = CF::PS, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* stage0 = reinterpret_cast<double*>(smem_raw);
+  double* red = stage0 + 2 * CF::STAGE;
+
+  const int e = blockIdx.x;
+  const int s0 = blockIdx.y * ST;
+  const int S = p.S;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int wm = w % CF::WM, wn = w / CF::WM;
+  const int g = lane >> 2, tg = lane & 3;
+  const int rb = p.row_ptr[e];
+  const int nb = p.row_ptr[e + 1] - rb;
+  const double* blocks = reinterpret_cast<const double*>(p.blocks);
+  const int nsh = min(ST, S - s0);  // shots of this tile
+
+  // Zero what cp.async never writes: K padding of B and X, and the X rows of
+  // shots beyond S, in both stages.
+  for (int st = 0; st < 2; ++st) {
+    double* B = stage0 + st * CF::STAGE;
+    double* X = B + CF::BSZ;
+    for (int i = t; i < (KP - R) * PS; i += CF::NT) B[R * PS + i] = 0.0;
+    if constexpr (PS > R) {
+      for (int i = t; i < ST * (PS - R); i += CF::NT) {
+        const int r = i / (PS - R), c = R + i % (PS - R);
+        X[r * PS + c] = 0.0;
+      }
+    }
+    for (int i = t; i < (ST - nsh) * R; i += CF::NT) {
+      const int r = nsh + i / R, c = i % R;
+      X[r * PS + c] = 0.0;
+    }
+  }
+
+  auto issue = [&](int b, int st) {
+    double* B = stage0 + st * CF::STAGE;
+    double* X = B + CF::BSZ;
+    const double* gb = blocks + size_t(rb + b) * R * p.bpitch;
+    for (int i = t; i < R * NP; i += CF::NT) {  // column k, 16-byte chunk j
+      const int k = i / NP, j = i - k * NP;
+      cp_async16(B + k * PS + 2 * j, gb + size_t(k) * p.bpitch + 2 * j);
+    }
+    const int c = p.col[rb + b];
+    const double* gx = p.x + (size_t(c) * S + s0) * R;
+    for (int i = t; i < nsh * NP; i += CF::NT) {
+      const int r = i / NP, j = i - r * NP;
+      cp_async16(X + r * PS + 2 * j, gx + size_t(r) * R + 2 * j);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+
+  double acc[MTW][NTW][2];
+#pragma unroll
+  for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+    for (int q = 0; q < NTW; ++q) acc[mt][q][0] = acc[mt][q][1] = 0.0;
+  // n-tiles of this warp that exist (warp-uniform).
+  const int nt0 = wn * NTW, ntn = min(NTW, NTL - nt0);
+
+  issue(0, 0);
+  for (int b = 0; b < nb; ++b) {
+    if (b + 1 < nb) {
+      issue(b + 1, (b + 1) & 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+    const double* B = stage0 + (b & 1) * CF::STAGE;
+    const double* X = B + CF::BSZ + (wm * MTW * 8 + g) * PS + tg;
+    const double* Bt = B + tg * PS + nt0 * 8 + g;
+#pragma unroll 1
+    for (int k0 = 0; k0 < KP; k0 += 4) {
+      double a[MTW], bb[NTW];
+#pragma unroll
+      for (int mt = 0; mt < MTW; ++mt) a[mt] = X[mt * 8 * PS + k0];
+#pragma unroll
+      for (int q = 0; q < NTW; ++q) bb[q] = (q < ntn) ? Bt[k0 * PS + q * 8] : 0.0;
+#pragma unroll
+      for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+        for (int q = 0; q < NTW; ++q)
+          if (q < ntn) dmma_m8n8k4(acc[mt][q][0], acc[mt][q][1], a[mt], bb[q]);
+    }
+    __syncthreads();
+  }
+
+  // ---- epilogue: thread holds rows (8(nt0+q) + 2tg, +1) of shots 8(wm*MTW + mt) + g ----
+  const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+  const double mi = p.minv[e];
+  const double dt = p.dt;
+  double en = 0.0;
+#pragma unroll
+  for (int mt = 0; mt < MTW; ++mt) {
+    const int sh = s0 + (wm * MTW + mt) * 8 + g;
+    if (sh >= S) continue;
+    const size_t me = (size_t(e) * S + sh) * R;
+    const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+    double Fk[2] = {0.0, 0.0};
+    if (is_src) {
+      Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
+      Fk[1] = p.F[(size_t(sh) * p.nF + k) * 2 + 1];
+    }
+#pragma unroll
+    for (int q = 0; q < NTW; ++q) {
+      const int r0 = (nt0 + q) * 8 + 2 * tg;
+      if (q >= ntn || r0 >= R) continue;  // rows come in pairs (R is even)
+      const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
+      const double2 up = p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
+      const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+      double un[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + h;
+        const int cmp = r / NP, ii = r - cmp * NP;
+        const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+        const double y = acc[mt][q][h];
+        if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
+        else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+        if (p.energy != nullptr) {
+          const double d = un[h] - u[h];
+          en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+        }
+      }
+      *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+    }
+  }
+
+  // ---- receivers ----
+  if (p.rcv_ptr != nullptr) {
+    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    if (q1 > q0) {
+      __syncthreads();  // this CTA's writes of u^{k+1} are visible after the barrier
+      const long long slot = k % p.seis_cap;
+      const int nwork = (q1 - q0) * ST * 2;
+      for (int wk = t; wk < nwork; wk += CF::NT) {
+        const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
+        const int sh = s0 + sl;
+        if (sh >= S) continue;
+        const int rid = p.rcv_id[q];
+        const double* ph = p.rcv_phi + size_t(rid) * NP;
+        const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+        double v = 0.0;
+        for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+        p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+      }
+    }
+  }
+
+  // ---- energy ----
+  if (p.energy != nullptr) {
+    const double v = warp_sum(en);
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int i = 0; i < CF::WARPS; ++i) sum += red[i];
+      atomicAdd(p.energy + (k % p.energy_cap), sum);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Batched FP32 step with asynchronous staging. Same GEMM as k_step_batched,
 // but the neighbours' states come from the FP32 transposed shadow written by
@@ -582,14 +794,6 @@ struct Batch32Cfg {
   }
 };
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
 
 template <int R>
 __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const StepParams p) {
