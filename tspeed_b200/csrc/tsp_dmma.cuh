@@ -9,9 +9,11 @@
 // multicast), so the consumer warps never wait on their own copies and the
 // next item's blocks arrive while the current item's epilogue runs.
 //
-// Roles: warps 0..NCW-1 consume (WM x WN warps, each MTW m-tiles of 8
-// shots x NTW n-tiles of 8 operator rows; accumulators in registers; they
-// also run the leap-frog epilogue, receivers and energy); warp NCW produces.
+// Roles: NG groups of NCW consumer warps (WM x WN warps, each MTW m-tiles
+// of 8 shots x NTW n-tiles of 8 operator rows; accumulators in registers;
+// they also run the leap-frog epilogue, receivers and energy); the groups
+// take the CTA's items in turn, so one group's epilogue overlaps the other's
+// products. The last warp produces.
 // Per block the producer issues two bulk copies: the operator block as it is
 // stored (column-major, pitch KP = R padded to 4, padding rows zero) and the
 // state tile of the neighbour (ST shot rows of R doubles, contiguous in the
@@ -36,15 +38,15 @@
 
 namespace tsp {
 
-template <int R, int NST_>
+template <int R, int NST_, int NG_>
 struct D64WCfg {
   static constexpr int KP = (R + 3) & ~3;  // also the stored block pitch of batched handles
   static constexpr int NTL = (R + 7) / 8;
   static constexpr int ST = R <= 42 ? 64 : 32;
-  static constexpr int WM = 4, WN = 2, NCW = WM * WN;
+  static constexpr int WM = 4, WN = 2, NCW = WM * WN, NG = NG_;
   static constexpr int MTW = ST / (8 * WM);
   static constexpr int NTW = (NTL + WN - 1) / WN;
-  static constexpr int NT = (NCW + 1) * 32;
+  static constexpr int NT = (NG * NCW + 1) * 32;
   static constexpr int NST = NST_;
   static constexpr int BSZ = KP * KP;      // doubles: operator stage [k][n], pitch KP
   static constexpr int XSZ = ST * R + 4;   // doubles: state stage [shot][k], pitch R, zero slack
@@ -54,9 +56,9 @@ struct D64WCfg {
   }
 };
 
-template <int R, int NST>
-__global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(const StepParams p, int* err_flag) {
-  typedef D64WCfg<R, NST> CF;
+template <int R, int NST, int NG>
+__global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, 1) k_step_batched64w(const StepParams p, int* err_flag) {
+  typedef D64WCfg<R, NST, NG> CF;
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* stages = reinterpret_cast<double*>(smem_raw);
@@ -83,7 +85,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(cons
   const long long G = gridDim.x;
   const double* blocks = reinterpret_cast<const double*>(p.blocks);
 
-  if (warp == CF::NCW) {
+  if (warp == NG * CF::NCW) {
     // ---------------- producer ----------------
     uint32_t j = 0;
     bool ok = true;
@@ -125,7 +127,8 @@ __global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(cons
     }
   } else {
     // ---------------- consumers ----------------
-    const int wm = warp % CF::WM, wn = warp / CF::WM;
+    const int grp = warp / CF::NCW, wl = warp % CF::NCW, tl = t - grp * CF::NCW * 32;
+    const int wm = wl % CF::WM, wn = wl / CF::WM;
     const int g = lane >> 2, tg = lane & 3;
     const int nt0 = wn * NTW, ntn = min(NTW, NTL - nt0);
     const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
@@ -133,10 +136,15 @@ __global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(cons
     double en = 0.0;
     uint32_t j = 0;
     bool dead = false;
-    for (long long item = blockIdx.x; item < nitems; item += G) {
+    long long it = 0;
+    for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
       const int e = int(item / ntile), tile = int(item % ntile);
       const int s0 = tile * ST;
       const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      if (int(it % NG) != grp) {  // another group's item: its stages, in producer order
+        j += uint32_t(nb);
+        continue;
+      }
       double acc[MTW][NTW][2];
 #pragma unroll
       for (int mt = 0; mt < MTW; ++mt)
@@ -215,11 +223,12 @@ __global__ void __launch_bounds__(D64WCfg<R, NST>::NT, 1) k_step_batched64w(cons
       if (p.rcv_ptr != nullptr) {
         const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
         if (q1 > q0) {
-          fx_epi_sync<CF::NCW * 32>();  // u^{k+1} of this item is visible to all consumers
+          // u^{k+1} of this item is visible to the whole group (barrier 1 + grp).
+          asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(CF::NCW * 32) : "memory");
           if (!dead) {
             const long long slot = k % p.seis_cap;
             const int nwork = (q1 - q0) * ST * 2;
-            for (int wk = t; wk < nwork; wk += CF::NCW * 32) {
+            for (int wk = tl; wk < nwork; wk += CF::NCW * 32) {
               const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
               const int sh = s0 + sl;
               if (sh >= S) continue;
