@@ -48,6 +48,12 @@ struct D64WCfg {
   static constexpr int NTW = (NTL + WN - 1) / WN;
   static constexpr int NT = (NG * NCW + 1) * 32;
   static constexpr int NST = NST_;
+  // A consumer waits on ring index j with the parity of use j / NST; the
+  // wait is unambiguous only if index j - NST has already been filled, i.e.
+  // if it was one of this group's own earlier blocks. Between two items of a
+  // group lie the other groups' items, at most 4 blocks each (a triangle has
+  // at most 3 neighbours), so the ring needs NST >= 4 (NG - 1) + 1 stages.
+  static_assert(NST_ >= 4 * (NG_ - 1) + 1, "ring too short for the consumer groups");
   static constexpr int BSZ = KP * KP;      // doubles: operator stage [k][n], pitch KP
   static constexpr int XSZ = ST * R + 4;   // doubles: state stage [shot][k], pitch R, zero slack
   static constexpr int STAGE = BSZ + XSZ;
