@@ -150,6 +150,22 @@ def estimate_dt(sim, cfl_fraction=0.4, iters=60):
     return cfl_fraction * 2.0 / math.sqrt(lmax), lmax
 
 
+# Nominal dense FP64 tensor-core rate of a B200 (DMMA); MEASURED_PEAKS.json
+# holds no FP64 figure.
+FP64_TENSOR_NOMINAL_TFLOPS = 40.0
+
+
+def fp64_tensor_roofline(nnzb, Np, nshots, ms_step, kernel):
+    """Roofline of the FP64 batched step against the FP64 tensor cores:
+    algorithmic flops 2 * nnzb * (2Np)^2 * shots per step."""
+    flops = 2.0 * nnzb * (2 * Np) ** 2 * nshots
+    ach = flops / (ms_step / 1e3) / 1e12
+    return {"bound": "tensor", "achieved": ach, "peak": FP64_TENSOR_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+            "frac": ach / FP64_TENSOR_NOMINAL_TFLOPS, "traffic": None, "kernel": kernel,
+            "peak_source": "nominal FP64 tensor rate (no FP64 figure measured by the driver)",
+            "algorithmic_flops_per_step": flops}
+
+
 def prepare(sim, prob, dt, nsteps):
     sim.set_dt(dt)
     for k, s in enumerate(prob.sources):
@@ -375,7 +391,8 @@ def main():
     algo = bytes_per_step(prob.mesh.ne, prob.Np, sim.nnzb, prob.nshots, form)
     achieved = algo / (ms_step / 1e3) / 1e9
     kernel = (KERNELS.get(variant, "batched") if variant is not None else
-              "k_step_rows<42>" if prob.nshots == 1 else "k_step_batched<42>")
+              "k_step_rows<42>" if prob.nshots == 1 else
+              "k_step_batched64w<42,5,2>" if args.precision == "fp64" else "k_step_batched<42>")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("bf16x3 fixed-point operator, f64 state" if form == "fx" else
@@ -392,6 +409,10 @@ def main():
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_step": algo},
             "gpu_launches": K + 1, "clocks": clocks}
+    if args.precision == "fp64" and prob.nshots > 1:
+        # The FP64 batched step is bound by the FP64 tensor cores (DMMA), not HBM.
+        line["roofline_hbm"] = line["roofline"]
+        line["roofline"] = fp64_tensor_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel)
     sim.close()
 
     if rank == 0 and world == 1 and not args.no_extras:
@@ -409,6 +430,20 @@ def main():
         line["plain_fp64_single_shot"] = {"value": v1, "unit": UNIT, "ms_per_step": ms1 / K,
                                           "roofline_frac": a1 / hbm, "achieved_gbs": a1}
         line["speedup_vs_plain_fp64"] = value / v1
+        # Exact FP64 for all shots: the FP64 tensor-core batched step.
+        if prob.nshots > 1 and args.precision != "fp64":
+            with capi.Simulation.from_problem(prob, precision="fp64") as s64:
+                prepare(s64, prob, dt, K + Wm + 2)
+                s64.first_step()
+                s64.run(Wm)
+                s64.run_timed(K)
+                ms64 = s64.run_timed(K)
+                nnzb64 = s64.nnzb
+            v64 = prob.nshots * dofs * K / (ms64 / 1e3)
+            line["batched_fp64"] = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / K,
+                                    "speedup_vs_plain_fp64": v64 / v1, "seismogram_err": "exact FP64",
+                                    "roofline": fp64_tensor_roofline(nnzb64, prob.Np, prob.nshots, ms64 / K,
+                                                                     "k_step_batched64w<42,5,2>")}
         # Accuracy of the measured form against FP64 over the full step count.
         nacc = prob.nsteps if args.accuracy_steps < 0 else args.accuracy_steps
         if args.precision != "fp64" and nacc > 0:

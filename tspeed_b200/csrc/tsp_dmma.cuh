@@ -136,6 +136,11 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, 1) k_step_batched64w(
     const int grp = warp / CF::NCW, wl = warp % CF::NCW, tl = t - grp * CF::NCW * 32;
     const int wm = wl % CF::WM, wn = wl / CF::WM;
     const int g = lane >> 2, tg = lane & 3;
+    // Fragment row g holds shot 8 mt + gs: rows 0..3 take the even shots and
+    // 4..7 the odd ones: with the state's shot pitch of R doubles, rows two
+    // shots apart are 4R words apart (168 = 8 mod 32 for 2Np = 42), so each
+    // half-warp's A loads fall in distinct banks.
+    const int gs = ((g & 3) << 1) | (g >> 2);
     const int nt0 = wn * NTW, ntn = min(NTW, NTL - nt0);
     const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
     const double dt = p.dt;
@@ -167,7 +172,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, 1) k_step_batched64w(
           continue;
         }
         const double* B = stages + size_t(s) * CF::STAGE;
-        const double* X = B + CF::BSZ + (wm * MTW * 8 + g) * R + tg;
+        const double* X = B + CF::BSZ + (wm * MTW * 8 + gs) * R + tg;
         const double* Bt = B + tg * KP + nt0 * 8 + g;
 #pragma unroll
         for (int k0 = 0; k0 < KP; k0 += 4) {
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, 1) k_step_batched64w(
         const double mi = p.minv[e];
 #pragma unroll
         for (int mt = 0; mt < MTW; ++mt) {
-          const int sh = s0 + (wm * MTW + mt) * 8 + g;
+          const int sh = s0 + (wm * MTW + mt) * 8 + gs;
           if (sh >= S) continue;
           const size_t me = (size_t(e) * S + sh) * R;
           const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
