@@ -62,8 +62,8 @@ struct D64WCfg {
   }
 };
 
-template <int R, int NST, int NG>
-__global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, 1) k_step_batched64w(const StepParams p, int* err_flag) {
+template <int R, int NST, int NG, int MINB = 1>
+__global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, MINB) k_step_batched64w(const StepParams p, int* err_flag) {
   typedef D64WCfg<R, NST, NG> CF;
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
