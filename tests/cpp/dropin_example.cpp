@@ -3,7 +3,8 @@
 // tspeed_gpu. Used by tests/test_gpu_cpp_dropin.py.
 //
 // usage: dropin_example mesh.msh rcv.txt outprefix N penalty dt nsteps sx sy f0 t0 amp dir
-//                       nreg [region lambda mu rho]...
+//                       nreg [region lambda mu rho]... [ba]
+// A trailing "ba" selects the BoundaryAdapted space (Examples/src/Lamb.cpp:26).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -29,7 +30,9 @@ int main(int argc, char** argv) {
   const int nreg = std::atoi(argv[a++]);
   try {
     Mesh_ptr Th(new Mesh(mesh));
-    FESpace_ptr Xh(new FESpace(Th, N));
+    const int nreg_args = 4 * nreg;
+    const bool ba = argc > a + nreg_args && std::string(argv[a + nreg_args]) == "ba";
+    FESpace_ptr Xh(new FESpace(Th, N, ba ? TSP_BASIS_BOUNDARY_ADAPTED : TSP_BASIS_DUBINER));
     Parameters p(Th);
     for (int r = 0; r < nreg; ++r) {
       const unsigned id = unsigned(std::atoi(argv[a++]));

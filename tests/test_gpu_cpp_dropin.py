@@ -15,7 +15,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 pytestmark = pytest.mark.gpu
 
 
-def test_cpp_dropin_matches_reference_golden(tmp_path):
+@pytest.mark.parametrize("case", ["g_n2_layers", "g_ba_n5"])
+def test_cpp_dropin_matches_reference_golden(case, tmp_path):
     cxx = shutil.which("g++") or shutil.which("c++")
     assert cxx, "no C++ compiler"
     exe = str(tmp_path / "dropin")
@@ -23,7 +24,11 @@ def test_cpp_dropin_matches_reference_golden(tmp_path):
     subprocess.run([cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
                     os.path.join(ROOT, "tests", "cpp", "dropin_example.cpp"), "-L" + lib, "-ltspeed_b200",
                     "-Wl,-rpath," + lib, "-o", exe], check=True)
-    g = load_golden("g_n2_layers")
+    g = load_golden(case)
+    ba = "basis" in g
+    # Tolerances as in test_gpu_parity.py: the BoundaryAdapted reference mass
+    # (condition number 1.1e5 at N = 5) amplifies rounding.
+    tol = 1e-11 if ba else 1e-12
     m = W.Mesh(g["xy"], g["tri"], g["region"], 0.0, 0.0)
     W.write_gmsh(str(tmp_path / "m.msh"), m)
     W.write_rcv(str(tmp_path / "m.rcv"), g["rcv"])
@@ -35,12 +40,14 @@ def test_cpp_dropin_matches_reference_golden(tmp_path):
     args = [exe, str(tmp_path / "m.msh"), str(tmp_path / "m.rcv"), str(tmp_path / "out"), str(int(g["N"])),
             repr(float(g["penalty"])), repr(float(g["dt"])), str(int(g["nsteps"])), repr(float(g["src"][0])),
             repr(float(g["src"][1])), repr(f0), repr(t0), repr(amp), str(int(sdir)), str(len(regions) // 4)] + regions
+    if ba:
+        args.append("ba")
     res = subprocess.run(args, check=True, capture_output=True, text=True)
     assert res.stdout.startswith(f"steps {int(g['nsteps'])} ")
     seis = np.stack([np.loadtxt(str(tmp_path / f"out_rcv_{i}.out")) for i in range(len(g["rcv"]))], 1)
     assert seis.shape == g["seis"].shape
     ok = np.isfinite(g["seis"])
-    assert rel(seis[ok], g["seis"][ok]) < 1e-12
+    assert rel(seis[ok], g["seis"][ok]) < tol
     # FESpace::points_out / field_out / L2error, host and device forms.
     n = int(g["nsteps"])
     assert (tmp_path / "out.points").read_bytes() == bytes(g["points_txt"])
@@ -51,4 +58,4 @@ def test_cpp_dropin_matches_reference_golden(tmp_path):
         assert got.shape == ref.shape
         assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-11 * scale)
     l2 = [float(v) for v in res.stdout.splitlines()[1].split()[1:]]
-    assert abs(l2[0] / float(g["l2_u"]) - 1) < 1e-12 and abs(l2[1] / float(g["l2_u"]) - 1) < 1e-12
+    assert abs(l2[0] / float(g["l2_u"]) - 1) < tol and abs(l2[1] / float(g["l2_u"]) - 1) < tol
