@@ -183,6 +183,16 @@ int dalloc(tsp_handle* h, T** p, size_t n) {
   return TSP_OK;
 }
 
+// A copy ordered on the handle's stream and complete on return. Plain
+// cudaMemcpy runs on the legacy default stream, which does not order against
+// the handles' non-blocking streams, and from pageable host memory it may
+// return before the data has reached the device.
+cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
+}
+
 // Stream-ordered release: work already queued on the handle's stream that
 // reads p completes first.
 void dfree(tsp_handle* h, void* p) {
@@ -789,7 +799,7 @@ void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* ds
 int check_device_error(tsp_handle* h) {
   if (!h->d_err) return TSP_OK;
   int v = 0;
-  TSP_CUDA(h, cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  TSP_CUDA(h, copy_sync(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (v) return fail(h, TSP_ERR_TIMEOUT, "a tensor-core step kernel timed out waiting for its MMAs; results invalid");
   return TSP_OK;
 }
@@ -1303,7 +1313,7 @@ int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double*
   if (v0 || h->d_v0) {
     if (!h->d_v0) {
       if ((rc = dalloc(h, &h->d_v0, nstate))) return rc;
-      TSP_CUDA(h, cudaMemset(h->d_v0, 0, nstate * sizeof(double)));
+      TSP_CUDA(h, cudaMemsetAsync(h->d_v0, 0, nstate * sizeof(double), h->stream));
     }
     if ((rc = put_shot(h, h->d_v0, shot, v0))) return rc;
   }
@@ -1551,14 +1561,14 @@ int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int6
   for (int lvl = 0; lvl < 2; ++lvl) {
     const double* src = lvl == 0 ? u_prev : u_cur;
     for (int s = 0; s < h->S; ++s) ref_to_dev(h, s, src + size_t(s) * nref, all.data());
-    TSP_CUDA(h, cudaMemcpy(lvl == 0 ? h->d_U[0] : h->d_U[1], all.data(), nstate * sizeof(double),
-                           cudaMemcpyHostToDevice));
+    TSP_CUDA(h, copy_sync(lvl == 0 ? h->d_U[0] : h->d_U[1], all.data(), nstate * sizeof(double),
+                          cudaMemcpyHostToDevice, h->stream));
   }
   if ((rc = refresh_shadow(h, 1))) return rc;
   h->steps_done = steps_done;
   h->last_time = last_time;
   long long sd = steps_done;
-  TSP_CUDA(h, cudaMemcpy(h->d_step, &sd, sizeof(sd), cudaMemcpyHostToDevice));
+  TSP_CUDA(h, copy_sync(h->d_step, &sd, sizeof(sd), cudaMemcpyHostToDevice, h->stream));
   clear_graphs(h);
   return TSP_OK;
 }
@@ -1594,7 +1604,7 @@ int tsp_apply(tsp_handle* h, const double* x, double* y) {
       std::memcpy(&v[size_t(e) * h->R + size_t(c) * h->Np], x + size_t(c) * h->ne * h->Np + size_t(e) * h->Np,
                   h->Np * sizeof(double));
   to_dev_coords(h, v.data(), 2ll * h->ne);  // B x = L (L^-1 B L^-T) (L^T x)
-  TSP_CUDA(h, cudaMemcpy(dx, v.data(), n1 * sizeof(double), cudaMemcpyHostToDevice));
+  TSP_CUDA(h, copy_sync(dx, v.data(), n1 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   if ((rc = launch_step(h, tsp::kModeApply, dx, nullptr, dy, 0, 1.0, h->stream))) return rc;
   TSP_CUDA(h, cudaGetLastError());
   TSP_CUDA(h, cudaMemcpyAsync(v.data(), dy, n1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1625,7 +1635,7 @@ int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax) {
     st ^= st << 17;
     x0[i] = double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
   }
-  TSP_CUDA(h, cudaMemcpy(da, x0.data(), nstate * sizeof(double), cudaMemcpyHostToDevice));
+  TSP_CUDA(h, copy_sync(da, x0.data(), nstate * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   double scale = 1.0, lam = 0.0;
   double acc[3];
   for (int it = 0; it < iters; ++it) {
@@ -1650,19 +1660,19 @@ int tsp_export_operator(tsp_handle* h, int32_t* row_ptr, int32_t* col, double* b
   int rc;
   if ((rc = begin(h))) return rc;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (row_ptr) TSP_CUDA(h, cudaMemcpy(row_ptr, h->d_row_ptr, (size_t(h->ne) + 1) * 4, cudaMemcpyDeviceToHost));
-  if (col) TSP_CUDA(h, cudaMemcpy(col, h->d_col, size_t(h->nnzb) * 4, cudaMemcpyDeviceToHost));
-  if (minv) TSP_CUDA(h, cudaMemcpy(minv, h->d_minv, size_t(h->ne) * 8, cudaMemcpyDeviceToHost));
+  if (row_ptr) TSP_CUDA(h, copy_sync(row_ptr, h->d_row_ptr, (size_t(h->ne) + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (col) TSP_CUDA(h, copy_sync(col, h->d_col, size_t(h->nnzb) * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (minv) TSP_CUDA(h, copy_sync(minv, h->d_minv, size_t(h->ne) * 8, cudaMemcpyDeviceToHost, h->stream));
   if (blocks) {
     const size_t RR = size_t(h->R) * h->R;
     const int BP = h->bpitch;
     const size_t esz = h->prec == TSP_PREC_FP64 ? 8 : (h->prec == TSP_PREC_FP32 ? 4 : 2);
     std::vector<unsigned char> raw(size_t(h->nnzb) * h->R * BP * esz);
     std::vector<float> sc;
-    TSP_CUDA(h, cudaMemcpy(raw.data(), h->d_blocks, raw.size(), cudaMemcpyDeviceToHost));
+    TSP_CUDA(h, copy_sync(raw.data(), h->d_blocks, raw.size(), cudaMemcpyDeviceToHost, h->stream));
     if (h->prec == TSP_PREC_BF16) {
       sc.resize(size_t(h->nnzb));
-      TSP_CUDA(h, cudaMemcpy(sc.data(), h->d_bscale, sc.size() * 4, cudaMemcpyDeviceToHost));
+      TSP_CUDA(h, copy_sync(sc.data(), h->d_bscale, sc.size() * 4, cudaMemcpyDeviceToHost, h->stream));
     }
     for (long long b = 0; b < h->nnzb; ++b)
       for (int c = 0; c < h->R; ++c)
@@ -2297,7 +2307,7 @@ int tsp_batch_estimate_lmax(tsp_batch* b, int32_t iters, double* lmax) {
       st ^= st << 17;
       x0[i] = double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
     }
-    if (cudaMemcpy(da, x0.data(), n1 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (copy_sync(da, x0.data(), n1 * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
       return bfail(b, TSP_ERR_CUDA, "upload of the start vector failed");
     std::vector<double> scale(nm, 1.0), acc(3 * size_t(nm)), lam(nm, 0.0);
     for (int it = 0; it < iters; ++it) {
@@ -2335,7 +2345,7 @@ int tsp_batch_set_dt(tsp_batch* b, const double* dt) {
       const int m = b->group_meshes[g][q];
       for (int e = 0; e < b->mesh_ne[m]; ++e) de[b->mesh_first[m] + e] = dt[m];
     }
-    if (cudaMemcpy(h->d_dt_elem, de.data(), de.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (copy_sync(h->d_dt_elem, de.data(), de.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
       return bfail(b, TSP_ERR_CUDA, "dt upload failed");
     h->dt = dt[b->group_meshes[g][0]];  // the handle's own dt is unused by its kernels
     h->dt_set = true;
@@ -2461,8 +2471,8 @@ int tsp_batch_get_u(tsp_batch* b, int32_t mesh, double* out) {
   cudaStreamSynchronize(b->stream);
   const int Np = h->Np, R = h->R, ne = b->mesh_ne[mesh];
   std::vector<double> v(size_t(ne) * R);
-  if (cudaMemcpy(v.data(), h->d_U[h->cur] + size_t(b->mesh_first[mesh]) * R, v.size() * sizeof(double),
-                 cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (copy_sync(v.data(), h->d_U[h->cur] + size_t(b->mesh_first[mesh]) * R, v.size() * sizeof(double),
+                cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
     return bfail(b, TSP_ERR_CUDA, "state read-back failed");
   for (int e = 0; e < ne; ++e)
     for (int c = 0; c < 2; ++c)
