@@ -5,15 +5,17 @@
 Workload (default): the 64-shot batched configuration -- 200x100 jittered
 squares (40,000 triangles), Dubiner N=5 (1.68 M DOFs per shot), per-element
 log-normal vp, 64 Ricker shots at seeded interior points, 128 surface
-receivers, dt = 0.4 x CFL from a device power iteration -- with FP32 operator
-blocks, FP32 accumulation and FP64 state. One bench "step" is one leap-frog
-step of all 64 shots. Under torchrun each rank runs its own 64 shots (weak
+receivers, dt = 0.4 x CFL from a device power iteration -- in exact FP64
+(FP64 operator blocks and state, the products on the FP64 tensor cores;
+--precision fp32 selects the FP32-operator form). One bench "step" is one
+leap-frog step of all 64 shots. Under torchrun each rank runs its own 64 shots (weak
 scaling, no collective in the data path); the timed region is bracketed by a
 barrier and a device synchronise, timed with CUDA events on the engine's
 stream, max over ranks.
 
 Also reported: the plain FP64 single-shot drop-in on the same mesh, the
-seismogram error of the measured form against FP64 over the full step count,
+FP32-operator batched form, the seismogram error of each form against FP64
+from the CUDA-core FP64 kernel over the full step count,
 an end-to-end number through the public C-ABI with host buffers, the
 roofline of the step kernel and the reference's CPU path on a bounded sample.
 """
@@ -150,6 +152,10 @@ def estimate_dt(sim, cfl_fraction=0.4, iters=60):
     return cfl_fraction * 2.0 / math.sqrt(lmax), lmax
 
 
+# The FP64 batched step kernel at 2Np = 42 (64-shot tiles, 5-stage ring, two
+# consumer groups, 8 x 1 warps per group).
+D64_KERNEL = "k_step_batched64w<42,5,2,1,8,1>"
+
 # Nominal dense FP64 tensor-core rate of a B200 (DMMA); MEASURED_PEAKS.json
 # holds no FP64 figure.
 FP64_TENSOR_NOMINAL_TFLOPS = 40.0
@@ -161,7 +167,7 @@ def fp64_tensor_roofline(nnzb, Np, nshots, ms_step, kernel):
     flops = 2.0 * nnzb * (2 * Np) ** 2 * nshots
     ach = flops / (ms_step / 1e3) / 1e12
     return {"bound": "tensor", "achieved": ach, "peak": FP64_TENSOR_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-            "frac": ach / FP64_TENSOR_NOMINAL_TFLOPS, "traffic": None, "kernel": kernel,
+            "frac": ach / FP64_TENSOR_NOMINAL_TFLOPS, "kernel": kernel,
             "peak_source": "nominal FP64 tensor rate (no FP64 figure measured by the driver)",
             "algorithmic_flops_per_step": flops}
 
@@ -316,9 +322,11 @@ def single_shot_forms(args):
 
 
 def config_dict(args, prob):
+    form = ("FP64 operator and state on the FP64 tensor cores (exact FP64)" if args.precision == "fp64" else
+            "FP32 operator / FP64 state, batched kernel chosen by the autotuner" if args.precision == "fp32" else
+            "BF16 operator / FP64 state")
     d = {"workload": "64-shot batched DG leap-frog: 200x100 jittered squares (40,000 triangles), Dubiner N=5, "
-                     "log-normal vp, 128 receivers, FP32 operator / FP64 state, batched kernel chosen by the "
-                     "autotuner",
+                     "log-normal vp, 128 receivers, " + form,
          "mesh_triangles": prob.mesh.ne if prob else 40000, "N": 5, "shots_per_gpu": args.nshots,
          "precision": args.precision, "dofs_per_shot": prob.dofs_per_shot if prob else 1680000,
          "l2": "inputs larger than L2 (state 0.86 GB per level, blocks 1.1 GB)", "parallelism": f"shots x{args.gpus}"}
@@ -331,7 +339,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16"])
     ap.add_argument("--nshots", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
@@ -392,7 +400,7 @@ def main():
     achieved = algo / (ms_step / 1e3) / 1e9
     kernel = (KERNELS.get(variant, "batched") if variant is not None else
               "k_step_rows<42>" if prob.nshots == 1 else
-              "k_step_batched64w<42,5,2>" if args.precision == "fp64" else "k_step_batched<42>")
+              D64_KERNEL if args.precision == "fp64" else "k_step_batched<42>")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("bf16x3 fixed-point operator, f64 state" if form == "fx" else
@@ -413,6 +421,10 @@ def main():
         # The FP64 batched step is bound by the FP64 tensor cores (DMMA), not HBM.
         line["roofline_hbm"] = line["roofline"]
         line["roofline"] = fp64_tensor_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel)
+        tr = captured_traffic(kernel, prob.mesh.ne, prob.nshots) if prob.N == 5 else None
+        line["roofline"]["traffic"] = tr
+        line["roofline"]["traffic_unit"] = "bytes per launch (ncu, profiles/traffic.json, scaled by element rows)"
+        line["roofline_hbm"]["traffic"] = tr
     sim.close()
 
     if rank == 0 and world == 1 and not args.no_extras:
@@ -430,6 +442,19 @@ def main():
         line["plain_fp64_single_shot"] = {"value": v1, "unit": UNIT, "ms_per_step": ms1 / K,
                                           "roofline_frac": a1 / hbm, "achieved_gbs": a1}
         line["speedup_vs_plain_fp64"] = value / v1
+        # Mixed precision for all shots: FP32 operator, autotuned batched kernel.
+        if prob.nshots > 1 and args.precision == "fp64":
+            with capi.Simulation.from_problem(prob, precision="fp32") as s32:
+                v32var = s32.kernel_variant
+                prepare(s32, prob, dt, K + Wm + 2)
+                s32.first_step()
+                s32.run(Wm)
+                s32.run_timed(K)
+                ms32 = s32.run_timed(K)
+            v32 = prob.nshots * dofs * K / (ms32 / 1e3)
+            line["batched_fp32_operator"] = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / K,
+                                             "speedup_vs_plain_fp64": v32 / v1,
+                                             "kernel": KERNELS.get(v32var, "batched"), "kernel_variant": v32var}
         # Exact FP64 for all shots: the FP64 tensor-core batched step.
         if prob.nshots > 1 and args.precision != "fp64":
             with capi.Simulation.from_problem(prob, precision="fp64") as s64:
@@ -443,22 +468,40 @@ def main():
             line["batched_fp64"] = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / K,
                                     "speedup_vs_plain_fp64": v64 / v1, "seismogram_err": "exact FP64",
                                     "roofline": fp64_tensor_roofline(nnzb64, prob.Np, prob.nshots, ms64 / K,
-                                                                     "k_step_batched64w<42,5,2>")}
-        # Accuracy of the measured form against FP64 over the full step count.
+                                                                     D64_KERNEL)}
+        # Accuracy of the measured form over the full step count against FP64
+        # computed by the CUDA-core FP64 kernel (TSP_BATCHED_VARIANT=2): for the
+        # FP64 tensor-core form this is the difference of two FP64 summation
+        # orders; for the mixed forms the precision error. With several shots
+        # the mixed FP32 form is reported too.
         nacc = prob.nsteps if args.accuracy_steps < 0 else args.accuracy_steps
-        if args.precision != "fp64" and nacc > 0:
+        if nacc > 0:
+            forms = [args.precision] + (["fp32"] if args.precision == "fp64" and prob.nshots > 1 else [])
             seis = {}
-            for prec in ("fp64", args.precision):
-                with capi.Simulation.from_problem(prob, precision=prec) as s:
-                    prepare(s, prob, dt, nacc)
-                    s.set_seismogram_capacity(nacc)
-                    s.first_step()
-                    s.run(nacc - 1)
-                    seis[prec] = s.seismograms(0, nacc)
-            ref = seis["fp64"]
-            err = float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))
-            line["seismogram_rel_l2_err_vs_fp64"] = err
+            for key, prec in [("ref", "fp64")] + [(f, f) for f in forms]:
+                old = os.environ.get("TSP_BATCHED_VARIANT")
+                if key == "ref":
+                    os.environ["TSP_BATCHED_VARIANT"] = "2"
+                try:
+                    with capi.Simulation.from_problem(prob, precision=prec) as s:
+                        prepare(s, prob, dt, nacc)
+                        s.set_seismogram_capacity(nacc)
+                        s.first_step()
+                        s.run(nacc - 1)
+                        seis[key] = s.seismograms(0, nacc)
+                finally:
+                    if key == "ref":
+                        if old is None:
+                            os.environ.pop("TSP_BATCHED_VARIANT", None)
+                        else:
+                            os.environ["TSP_BATCHED_VARIANT"] = old
+            ref = seis["ref"]
+            errs = {f: float(np.linalg.norm(seis[f] - ref) / np.linalg.norm(ref)) for f in forms}
+            line["seismogram_rel_l2_err_vs_fp64"] = errs[args.precision]
+            line["accuracy_reference"] = "FP64, CUDA-core batched kernel (TSP_BATCHED_VARIANT=2)"
             line["accuracy_steps"] = nacc
+            if "batched_fp32_operator" in line:
+                line["batched_fp32_operator"]["seismogram_rel_l2_err_vs_fp64"] = errs["fp32"]
         # End to end through the public C-ABI with host buffers.
         ne_steps = K
         t0 = time.perf_counter()

@@ -38,12 +38,12 @@
 
 namespace tsp {
 
-template <int R, int NST_, int NG_>
+template <int R, int NST_, int NG_, int WM_ = 4, int WN_ = 2>
 struct D64WCfg {
   static constexpr int KP = (R + 3) & ~3;  // also the stored block pitch of batched handles
   static constexpr int NTL = (R + 7) / 8;
   static constexpr int ST = R <= 42 ? 64 : 32;
-  static constexpr int WM = 4, WN = 2, NCW = WM * WN, NG = NG_;
+  static constexpr int WM = WM_, WN = WN_, NCW = WM * WN, NG = NG_;
   static constexpr int MTW = ST / (8 * WM);
   static constexpr int NTW = (NTL + WN - 1) / WN;
   static constexpr int NT = (NG * NCW + 1) * 32;
@@ -62,9 +62,10 @@ struct D64WCfg {
   }
 };
 
-template <int R, int NST, int NG, int MINB = 1>
-__global__ void __launch_bounds__(D64WCfg<R, NST, NG>::NT, MINB) k_step_batched64w(const StepParams p, int* err_flag) {
-  typedef D64WCfg<R, NST, NG> CF;
+template <int R, int NST, int NG, int MINB = 1, int WM = 4, int WN = 2>
+__global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
+    k_step_batched64w(const StepParams p, int* err_flag) {
+  typedef D64WCfg<R, NST, NG, WM, WN> CF;
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* stages = reinterpret_cast<double*>(smem_raw);
