@@ -329,7 +329,9 @@ def config_dict(args, prob):
                      "log-normal vp, 128 receivers, " + form,
          "mesh_triangles": prob.mesh.ne if prob else 40000, "N": 5, "shots_per_gpu": args.nshots,
          "precision": args.precision, "dofs_per_shot": prob.dofs_per_shot if prob else 1680000,
-         "l2": "inputs larger than L2 (state 0.86 GB per level, blocks 1.1 GB)", "parallelism": f"shots x{args.gpus}"}
+         "l2": "inputs larger than L2 (state 0.86 GB per level, blocks %s GB)" %
+               {"fp64": "2.25", "fp32": "1.1", "bf16": "0.56"}[args.precision],
+         "parallelism": f"shots x{args.gpus}"}
     return d
 
 
