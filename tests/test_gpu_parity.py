@@ -596,7 +596,7 @@ def test_golden_projection_on_the_device(golden):
     assert rel(u1, ref1) < tol
 
 
-@pytest.mark.parametrize("N", [1, 3, 5, 6])
+@pytest.mark.parametrize("N", [1, 3, 5, 6, 7, 8])
 def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
     """FP64 with several shots runs on the FP64 tensor cores (DMMA): the
     warp-specialised persistent kernel (default) and the single-role one

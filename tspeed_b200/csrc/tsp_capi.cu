@@ -501,8 +501,11 @@ template <int R>
 int launch_d64w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   // Each consumer warp owns one m-tile of 8 shots and every operator row
   // (all n-tiles) when the tile has 64 shots: measured fastest at 2Np = 42
-  // (1.55 ms per step against 1.71 for 2 m-tiles x half the rows).
-  constexpr int NST = 5, NG = 2;
+  // (1.55 ms per step against 1.71 for 2 m-tiles x half the rows). For
+  // 2Np > 56 a stage no longer fits five times in shared memory: one consumer
+  // group with a 3-stage (2Np = 72) or 2-stage (2Np = 90) ring.
+  constexpr int NG = R <= 56 ? 2 : 1;
+  constexpr int NST = R <= 56 ? 5 : (R <= 72 ? 3 : 2);
   constexpr int WM = tsp::D64WCfg<R, NST, NG>::ST / 8, WN = 8 / WM;
   typedef tsp::D64WCfg<R, NST, NG, WM, WN> CF;
   const size_t smem = CF::smem_bytes();
@@ -643,11 +646,9 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   // FP64 with several shots: the FP64 tensor-core (DMMA) kernels, the
   // warp-specialised persistent one by default; TSP_BATCHED_VARIANT=3 selects
   // the single-role DMMA kernel and 2 the register-staged CUDA-core kernel.
-  if constexpr (R <= 56) {
-    if (h->S > 1 && h->prec == TSP_PREC_FP64 && h->kernel_variant != 2 &&
-        (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
-      return h->kernel_variant == 3 ? launch_d64<R>(h, p, st) : launch_d64w<R>(h, p, st);
-  }
+  if (h->S > 1 && h->prec == TSP_PREC_FP64 && h->kernel_variant != 2 &&
+      (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
+    return h->kernel_variant == 3 ? launch_d64<R>(h, p, st) : launch_d64w<R>(h, p, st);
   if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::BatchCfg<R> CF;
     const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
