@@ -161,15 +161,32 @@ D64_KERNEL = "k_step_batched64w<42,5,2,1,8,1>"
 FP64_TENSOR_NOMINAL_TFLOPS = 40.0
 
 
-def fp64_tensor_roofline(nnzb, Np, nshots, ms_step, kernel):
+_FP64_PEAK = {}
+
+
+def fp64_tensor_peak(device):
+    """FP64 tensor-core rate measured on this GPU (register-only DMMA loop in
+    the library, tsp_fp64_tensor_peak); MEASURED_PEAKS.json has no FP64 figure."""
+    if device not in _FP64_PEAK:
+        try:
+            _FP64_PEAK[device] = capi.fp64_tensor_peak(device)
+        except Exception:
+            _FP64_PEAK[device] = None
+    return _FP64_PEAK[device]
+
+
+def fp64_tensor_roofline(nnzb, Np, nshots, ms_step, kernel, device=0):
     """Roofline of the FP64 batched step against the FP64 tensor cores:
     algorithmic flops 2 * nnzb * (2Np)^2 * shots per step."""
     flops = 2.0 * nnzb * (2 * Np) ** 2 * nshots
     ach = flops / (ms_step / 1e3) / 1e12
-    return {"bound": "tensor", "achieved": ach, "peak": FP64_TENSOR_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-            "frac": ach / FP64_TENSOR_NOMINAL_TFLOPS, "kernel": kernel,
-            "peak_source": "nominal FP64 tensor rate (no FP64 figure measured by the driver)",
-            "algorithmic_flops_per_step": flops}
+    meas = fp64_tensor_peak(device)
+    peak = meas if meas else FP64_TENSOR_NOMINAL_TFLOPS
+    src = ("measured on this GPU: register-only DMMA loop (tsp_fp64_tensor_peak)" if meas else
+           "nominal FP64 tensor rate (probe unavailable)")
+    return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "kernel": kernel, "peak_source": src, "peak_nominal": FP64_TENSOR_NOMINAL_TFLOPS,
+            "frac_of_nominal": ach / FP64_TENSOR_NOMINAL_TFLOPS, "algorithmic_flops_per_step": flops}
 
 
 def prepare(sim, prob, dt, nsteps):
@@ -422,7 +439,7 @@ def main():
     if args.precision == "fp64" and prob.nshots > 1:
         # The FP64 batched step is bound by the FP64 tensor cores (DMMA), not HBM.
         line["roofline_hbm"] = line["roofline"]
-        line["roofline"] = fp64_tensor_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel)
+        line["roofline"] = fp64_tensor_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel, local_rank)
         tr = captured_traffic(kernel, prob.mesh.ne, prob.nshots) if prob.N == 5 else None
         line["roofline"]["traffic"] = tr
         line["roofline"]["traffic_unit"] = "bytes per launch (ncu, profiles/traffic.json, scaled by element rows)"

@@ -152,6 +152,11 @@ int tsp_create_from_blocks(const tsp_block_problem* prob, tsp_handle** out);
 /* Releases every resource of the handle. NULL is accepted. */
 int tsp_destroy(tsp_handle* h);
 
+/* FP64 tensor-core (DMMA) throughput of a device in TFLOP/s, measured by a
+ * register-only loop of a few milliseconds: the FP64 roofline denominator
+ * that bench.py reports (no counterpart in the reference). */
+int tsp_fp64_tensor_peak(int32_t device, double* tflops);
+
 /* Device memory of all handles comes from one stream-ordered pool per
  * device that keeps freed memory cached for the process, so creating a
  * simulation after destroying another does not pay for multi-GB device

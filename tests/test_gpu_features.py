@@ -190,3 +190,11 @@ def test_pooled_allocations_are_reused_and_released():
         s.first_step()
         s.run(59)
         assert np.array_equal(s.seismograms(0, 60), out[0])
+
+
+def test_fp64_tensor_peak_probe():
+    """The FP64 tensor-core throughput probe behind the benchmark's FP64
+    roofline returns a plausible B200 rate (nominal 40 TFLOP/s)."""
+    v = capi.fp64_tensor_peak(0)
+    print("FP64 tensor peak", v)
+    assert 10.0 < v < 60.0

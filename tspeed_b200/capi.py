@@ -98,6 +98,7 @@ SIGNATURES = {
     "tsp_points_out": (C.c_int, [C.c_int32, _dp, C.c_int32, _ip, C.c_char_p]),
     "tsp_set_initial_values": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "tsp_release_cached_memory": (C.c_int, [C.c_int32]),
+    "tsp_fp64_tensor_peak": (C.c_int, [C.c_int32, _dp]),
     "tsp_locate_points": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int32, _ip, C.c_int32, _dp, _ip, _dp]),
     "tsp_eval_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
     "tsp_quadrature_rule": (C.c_int, [C.c_int32, _dp, _dp]),
@@ -216,6 +217,13 @@ def quadrature_rule(N: int):
     r, w = np.zeros(((N + 1) ** 2, 2)), np.zeros((N + 1) ** 2)
     _check(lib().tsp_quadrature_rule(N, _d(r), _d(w)))
     return r, w
+
+
+def fp64_tensor_peak(device: int = 0) -> float:
+    """Measured FP64 tensor-core (DMMA) throughput, TFLOP/s."""
+    v = C.c_double()
+    _check(lib().tsp_fp64_tensor_peak(device, C.byref(v)))
+    return v.value
 
 
 def release_cached_memory(device: int = 0):

@@ -1970,6 +1970,45 @@ int tsp_quadrature_rule(int32_t N, double* rpts, double* w) {
   return TSP_OK;
 }
 
+namespace {
+__device__ double g_peak_sink;
+}  // namespace
+
+int tsp_fp64_tensor_peak(int32_t device, double* tflops) {
+  if (!tflops) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  int prev = 0, sms = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  double* sink = nullptr;
+  if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void**>(&sink), g_peak_sink);
+  float ms = 0.0f;
+  const int grid = 4 * sms, threads = 512, iters = 1024;
+  if (e == cudaSuccess) {
+    tsp::k_fp64_tensor_peak<<<grid, threads, 0, st>>>(sink, 16);  // warm-up
+    e = cudaEventRecord(e0, st);
+    tsp::k_fp64_tensor_peak<<<grid, threads, 0, st>>>(sink, iters);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(nullptr, TSP_ERR_CUDA, std::string("FP64 tensor probe: ") + cudaGetErrorString(e));
+  // 8 DMMAs of 8 x 8 x 4 multiply-adds per warp and iteration.
+  const double flops = 2.0 * 256.0 * 8.0 * iters * double(grid) * (threads / 32);
+  *tflops = flops / (double(ms) * 1e-3) / 1e12;
+  return TSP_OK;
+}
+
 int tsp_get_ref_invmass(const tsp_handle* h, int32_t* basis, double* out) {
   if (!h) return TSP_ERR_ARG;
   if (basis) *basis = h->basis;

@@ -609,6 +609,24 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
                : "d"(a), "d"(b));
 }
 
+// FP64 tensor-core throughput probe for the benchmark's roofline: every warp
+// runs 8 independent DMMA accumulation chains on register operands, nothing
+// is read from memory; the result is written only under a condition that
+// never holds, so the loop is not removed.
+__global__ void k_fp64_tensor_peak(double* sink, int iters) {
+  double c[8][2];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c[j][0] = c[j][1] = 0.0;
+  const double a = 1e-3 * (threadIdx.x + 1), b = 1.0 + 1e-9 * blockIdx.x;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dmma_m8n8k4(c[j][0], c[j][1], a, b);
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += c[j][0] + c[j][1];
+  if (s == -1.0) *sink = s;
+}
+
 template <int R>
 __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const StepParams p) {
   typedef D64Cfg<R> CF;
