@@ -152,6 +152,13 @@ int tsp_create_from_blocks(const tsp_block_problem* prob, tsp_handle** out);
 /* Releases every resource of the handle. NULL is accepted. */
 int tsp_destroy(tsp_handle* h);
 
+/* Self-test of the bounded wait used by the warp-specialised kernels (no
+ * counterpart in the reference): a kernel waits on a barrier phase that
+ * nothing completes; the wait gives up after about a second, raises the
+ * kernel's abort flag and the kernel ends normally. Expected: *completed = 0,
+ * *abort_raised = 1, TSP_OK, and the device stays usable. */
+int tsp_selftest_bounded_wait(int32_t device, int32_t* completed, int32_t* abort_raised);
+
 /* FP64 tensor-core (DMMA) throughput of a device in TFLOP/s, measured by a
  * register-only loop of a few milliseconds: the FP64 roofline denominator
  * that bench.py reports (no counterpart in the reference). */

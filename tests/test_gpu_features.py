@@ -198,3 +198,22 @@ def test_fp64_tensor_peak_probe():
     v = capi.fp64_tensor_peak(0)
     print("FP64 tensor peak", v)
     assert 10.0 < v < 60.0
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable():
+    """Failure detection on the device without a fault: a wait on a barrier
+    phase that nothing completes gives up after its limit (about a second),
+    raises the abort flag, the kernel ends normally, and a simulation runs
+    on the same device right after."""
+    completed, aborted = capi.selftest_bounded_wait(0)
+    assert completed == 0 and aborted == 1
+    m = W.jittered_rect(3, 2, 300.0, 200.0, seed=5)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    with capi.Simulation.create(m.xy, m.tri, 2, lam, mu, rho, [(150.0, 100.0), (80.0, 60.0)], [],
+                                penalty=10.0) as s:
+        s.set_dt(1e-4)
+        s.set_ricker(0, 20.0, 0.05, -1.0, 1, 10)
+        s.set_ricker(1, 20.0, 0.05, -1.0, 1, 10)
+        s.first_step()
+        s.run(9)
+        assert s.check_finite()

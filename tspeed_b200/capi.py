@@ -99,6 +99,7 @@ SIGNATURES = {
     "tsp_set_initial_values": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
     "tsp_release_cached_memory": (C.c_int, [C.c_int32]),
     "tsp_fp64_tensor_peak": (C.c_int, [C.c_int32, _dp]),
+    "tsp_selftest_bounded_wait": (C.c_int, [C.c_int32, _ip, _ip]),
     "tsp_locate_points": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, C.c_int32, _ip, C.c_int32, _dp, _ip, _dp]),
     "tsp_eval_basis": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
     "tsp_quadrature_rule": (C.c_int, [C.c_int32, _dp, _dp]),
@@ -217,6 +218,13 @@ def quadrature_rule(N: int):
     r, w = np.zeros(((N + 1) ** 2, 2)), np.zeros((N + 1) ** 2)
     _check(lib().tsp_quadrature_rule(N, _d(r), _d(w)))
     return r, w
+
+
+def selftest_bounded_wait(device: int = 0):
+    """(completed, abort_raised) of a kernel whose bounded wait must time out."""
+    c, a = C.c_int32(), C.c_int32()
+    _check(lib().tsp_selftest_bounded_wait(device, C.byref(c), C.byref(a)))
+    return c.value, a.value
 
 
 def fp64_tensor_peak(device: int = 0) -> float:

@@ -1974,6 +1974,31 @@ namespace {
 __device__ double g_peak_sink;
 }  // namespace
 
+int tsp_selftest_bounded_wait(int32_t device, int32_t* completed, int32_t* abort_raised) {
+  if (!completed || !abort_raised) return fail(nullptr, TSP_ERR_ARG, "null argument");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  cudaStream_t st = nullptr;
+  int* d = nullptr;
+  int h[3] = {-1, -1, -1};
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&d), 3 * sizeof(int), st);
+  if (e == cudaSuccess) {
+    tsp::k_selftest_bounded_wait<<<1, 32, 0, st>>>(d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (d) cudaFreeAsync(d, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (st) cudaStreamDestroy(st);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(nullptr, TSP_ERR_CUDA, std::string("bounded-wait self-test: ") + cudaGetErrorString(e));
+  *completed = h[0];
+  *abort_raised = h[1];
+  return TSP_OK;
+}
+
 int tsp_fp64_tensor_peak(int32_t device, double* tflops) {
   if (!tflops) return fail(nullptr, TSP_ERR_ARG, "null argument");
   int prev = 0, sms = 0;

@@ -264,4 +264,26 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
   if (t == 0 && *abort_s) atomicExch(err_flag, 1);
 }
 
+// Self-test of the bounded mbarrier wait that every warp-specialised kernel
+// here relies on: one thread waits on a phase that nothing completes. The
+// wait must give up after its limit (about a second), raise the abort flag
+// and let the kernel end normally, leaving the context usable.
+__global__ void k_selftest_bounded_wait(int* out) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_s;
+  if (threadIdx.x == 0) {
+    abort_s = 0;
+    fx_mbar_init(smem_u32(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const long long t0 = clock64();
+    const bool ok = fx_wait(smem_u32(&bar), 0, &abort_s);
+    out[0] = ok ? 1 : 0;
+    out[1] = abort_s;
+    out[2] = int((clock64() - t0) >> 20);  // waited cycles / 2^20
+  }
+}
+
 }  // namespace tsp
