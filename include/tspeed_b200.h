@@ -217,8 +217,10 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
 /* Kernel variant of the batched FP32 step chosen for this handle by the
  * autotuner at creation (or forced by TSP_BATCHED_VARIANT): 0 K-split /
  * pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel, 2 non-persistent
- * CUDA-core kernel, 4 tensor-core fixed-point kernel. No counterpart in the
- * reference (its step is a single CPU path). */
+ * CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64 handles with
+ * several shots: 5 warp-specialised FP64 tensor-core (DMMA) kernel (default),
+ * 3 single-role DMMA kernel, 2 CUDA-core kernel (3 and 2 when forced). No
+ * counterpart in the reference (its step is a single CPU path). */
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant);
 
 /* Number of leap-frog steps done (first_step counts as 1) and the

@@ -628,6 +628,7 @@ def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
             s.first_step()
             s.run(n - 1)
             out[variant] = (s.seismograms(0, n), s.u_all(), s.energy(1, n - 1))
+            assert s.kernel_variant == {"auto": 5, "3": 3, "2": 2}[variant]
     for v in ("auto", "3"):
         for i in range(3):
             print("N", N, v, i, rel(out[v][i], out["2"][i]))

@@ -364,7 +364,9 @@ class Simulation:
     @property
     def kernel_variant(self) -> int:
         """Batched-step kernel chosen by the autotuner (or TSP_BATCHED_VARIANT):
-        0/1/2 CUDA-core kernels, 4 tensor-core fixed-point kernel."""
+        FP32: 0/1/2 CUDA-core kernels, 4 tensor-core fixed-point kernel; FP64
+        with several shots: 5 warp-specialised FP64 tensor-core kernel, 3
+        single-role one, 2 CUDA-core kernel."""
         v = C.c_int32()
         _check(lib().tsp_get_kernel_variant(self._h, C.byref(v)), self._h)
         return v.value

@@ -1429,6 +1429,11 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant) {
   if (!h || !variant) return TSP_ERR_ARG;
   *variant = h->kernel_variant;
+  // FP64 with several shots: 2 CUDA-core, 3 single-role DMMA, else the
+  // warp-specialised DMMA kernel, reported as 5.
+  if (h->prec == TSP_PREC_FP64 && h->S > 1 && h->op_kind == TSP_OP_EXPLICIT && h->kernel_variant != 2 &&
+      h->kernel_variant != 3)
+    *variant = 5;
   return TSP_OK;
 }
 
