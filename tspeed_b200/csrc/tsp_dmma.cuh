@@ -4,16 +4,20 @@
 // The same product as k_step_batched64d -- per work item (element row e,
 // tile of ST shots) Y[shot][r] = sum_b sum_k X_{col b}[shot][k] B_b[r][k]
 // with mma.sync m8n8k4 .f64 (exact FP64 products, FP64 accumulation) -- but
-// the operands stream through an NST-stage ring in shared memory filled by a
-// producer warp with bulk copies (cp.async.bulk, completion on mbarriers, no
-// multicast), so the consumer warps never wait on their own copies and the
-// next item's blocks arrive while the current item's epilogue runs.
+// the operands stream through shared-memory rings (NSG stages per consumer
+// group) filled by producer lanes with bulk copies (cp.async.bulk, completion
+// on mbarriers, no multicast), so the consumer warps never wait on their own
+// copies and the next item's blocks arrive while the current item's epilogue
+// runs.
 //
 // Roles: NG groups of NCW consumer warps (WM x WN warps, each MTW m-tiles
 // of 8 shots x NTW n-tiles of 8 operator rows; accumulators in registers;
 // they also run the leap-frog epilogue, receivers and energy); the groups
 // take the CTA's items in turn, so one group's epilogue overlaps the other's
-// products. The last warp produces.
+// products. The last warp produces: its lane g fills group g's ring.
+// The epilogue reads u^k from the diagonal block's state stage (the
+// element's own tile, already in shared memory) and u^{k-1} through loads
+// issued before the item's products, so it waits on no global load.
 // Per block the producer issues two bulk copies: the operator block as it is
 // stored (column-major, pitch KP = R padded to 4, padding rows zero) and the
 // state tile of the neighbour (ST shot rows of R doubles, contiguous in the
@@ -38,7 +42,7 @@
 
 namespace tsp {
 
-template <int R, int NST_, int NG_, int WM_ = 4, int WN_ = 2>
+template <int R, int NSG_, int NG_, int WM_ = 4, int WN_ = 2>
 struct D64WCfg {
   static constexpr int KP = (R + 3) & ~3;  // also the stored block pitch of batched handles
   static constexpr int NTL = (R + 7) / 8;
@@ -47,30 +51,52 @@ struct D64WCfg {
   static constexpr int MTW = ST / (8 * WM);
   static constexpr int NTW = (NTL + WN - 1) / WN;
   static constexpr int NT = (NG * NCW + 1) * 32;
-  static constexpr int NST = NST_;
-  // A consumer waits on ring index j with the parity of use j / NST; the
-  // wait is unambiguous only if index j - NST has already been filled, i.e.
-  // if it was one of this group's own earlier blocks. Between two items of a
-  // group lie the other groups' items, at most 4 blocks each (a triangle has
-  // at most 3 neighbours), so the ring needs NST >= 4 (NG - 1) + 1 stages.
-  static_assert(NST_ >= 4 * (NG_ - 1) + 1, "ring too short for the consumer groups");
+  // Each consumer group has a ring of its own (NSG stages), filled by its own
+  // producer lane in the group's block order. A consumer waits on its ring
+  // index j with the parity of use j / NSG: index j - NSG of the same ring is
+  // the group's own block, consumed (hence landed) before, and use j + NSG
+  // cannot be issued before this group releases j, so the barrier has
+  // completed either j / NSG or j / NSG + 1 uses and the parity names the
+  // right one -- whatever the row lengths and the ring length. (A ring shared
+  // by the groups does not have this property: a group's index j - NST may
+  // belong to another group's copy that is still in flight, and bulk copies
+  // complete in any order.)
+  static constexpr int NSG = NSG_;
+  static constexpr int NST = NG * NSG;     // stages in total
+  static_assert(NSG_ >= 1 && NG_ >= 1, "ring");
   static constexpr int BSZ = KP * KP;      // doubles: operator stage [k][n], pitch KP
   static constexpr int XSZ = ST * R + 4;   // doubles: state stage [shot][k], pitch R, zero slack
   static constexpr int STAGE = BSZ + XSZ;
+  static_assert(BSZ % 2 == 0 && STAGE % 2 == 0, "16-byte aligned stages");
   static constexpr size_t smem_bytes() {
     return size_t(NST) * STAGE * sizeof(double) + size_t(2 * NST) * sizeof(uint64_t) + 16;
   }
 };
 
-template <int R, int NST, int NG, int MINB = 1, int WM = 4, int WN = 2>
-__global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
+// Stages per group ring that fit in shared memory (at most CAP).
+template <int R, int NG, int WM, int WN, int CAP>
+constexpr int d64w_fit_nsg() {
+  constexpr size_t one = D64WCfg<R, 1, NG, WM, WN>::smem_bytes();
+  constexpr size_t budget = 227 * 1024;
+  return int(budget / one) >= CAP ? CAP : int(budget / one);
+}
+
+// EPI selects where the epilogue gets u^k and u^{k-1}: 0 global loads issued
+// by the epilogue (fewest registers: the two consumer groups hide the
+// latency behind each other's products); 1 u^k from the diagonal block's
+// state stage and u^{k-1} requested before the products (no load latency in
+// the epilogue; 24 more registers per thread at 2Np = 42 with all rows per
+// warp, so it suits warp tiles of half the rows and a single group).
+template <int R, int NSG, int NG, int MINB = 1, int WM = 4, int WN = 2, int EPI = 0>
+__global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
     k_step_batched64w(const StepParams p, int* err_flag) {
-  typedef D64WCfg<R, NST, NG, WM, WN> CF;
+  typedef D64WCfg<R, NSG, NG, WM, WN> CF;
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
+  constexpr int NST = CF::NST;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* stages = reinterpret_cast<double*>(smem_raw);
-  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NST] stage landed
-  uint64_t* bempty = bfull + NST;                                                    // [NST] stage consumed
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NG][NSG] stage landed
+  uint64_t* bempty = bfull + NST;                                                    // [NG][NSG] stage consumed
   volatile int* abort_s = reinterpret_cast<volatile int*>(bempty + NST);
 
   if (*reinterpret_cast<volatile int*>(err_flag) != 0) return;  // an earlier launch of the run timed out
@@ -93,41 +119,43 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
   const double* blocks = reinterpret_cast<const double*>(p.blocks);
 
   if (warp == NG * CF::NCW) {
-    // ---------------- producer ----------------
-    uint32_t j = 0;
-    bool ok = true;
-    for (long long item = blockIdx.x; item < nitems && ok; item += G) {
-      const int e = int(item / ntile), tile = int(item % ntile);
-      const int s0 = tile * ST, nsh = min(ST, S - s0);
-      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
-      const uint32_t bbytes = uint32_t(R) * KP * 8, xbytes = uint32_t(nsh) * R * 8;
-      for (int b = 0; b < nb; ++b) {
-        const int s = int(j % NST);
-        const uint32_t n = j / NST;
-        int okl = 1;
-        if (lane == 0 && n > 0) okl = fx_wait(smem_u32(&bempty[s]), (n - 1) & 1, abort_s) ? 1 : 0;
-        if (!__shfl_sync(0xffffffffu, okl, 0)) {
-          ok = false;
-          break;
-        }
-        if (lane == 0) {
+    // ---------------- producers: lane g fills ring g ----------------
+    if (lane < NG) {
+      const int g = lane;
+      uint64_t* gfull = bfull + g * NSG;
+      uint64_t* gempty = bempty + g * NSG;
+      double* gst = stages + size_t(g) * NSG * CF::STAGE;
+      uint32_t j = 0;
+      bool ok = true;
+      for (long long item = blockIdx.x + g * G; item < nitems && ok; item += NG * G) {
+        const int e = int(item / ntile), tile = int(item % ntile);
+        const int s0 = tile * ST, nsh = min(ST, S - s0);
+        const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+        const uint32_t bbytes = uint32_t(R) * KP * 8, xbytes = uint32_t(nsh) * R * 8;
+        for (int b = 0; b < nb; ++b) {
+          const int s = int(j % NSG);
+          const uint32_t n = j / NSG;
+          if (n > 0 && !fx_wait(smem_u32(&gempty[s]), (n - 1) & 1, abort_s)) {
+            ok = false;
+            break;
+          }
           const int c = p.col[rb + b];
-          const uint32_t bar = smem_u32(&bfull[s]);
-          const uint32_t dB = smem_u32(stages + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 8;
+          const uint32_t bar = smem_u32(&gfull[s]);
+          const uint32_t dB = smem_u32(gst + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 8;
           fx_mbar_arrive_tx(bar, bbytes + xbytes);
           fx_bulk_g2s(dB, blocks + size_t(rb + b) * R * KP, bbytes, bar);
           fx_bulk_g2s(dX, p.x + (size_t(c) * S + s0) * R, xbytes, bar);
+          ++j;
         }
-        ++j;
       }
-    }
-    // Every issued copy lands before the CTA ends (bounded; copies complete).
-    if (lane == 0) {
+      // Every issued copy lands before the CTA ends (bounded; copies
+      // complete). At most one use of a stage is in flight: use u is issued
+      // only after use u - 1 was consumed.
       const long long t0 = clock64();
-      for (int s = 0; s < NST; ++s) {
+      for (int s = 0; s < NSG; ++s) {
         if (j <= uint32_t(s)) continue;
-        const uint32_t uses = (j - 1 - s) / NST + 1;
-        while (!mbar_try(smem_u32(&bfull[s]), (uses - 1) & 1) && clock64() - t0 < (1ll << 31)) {
+        const uint32_t uses = (j - 1 - s) / NSG + 1;
+        while (!mbar_try(smem_u32(&gfull[s]), (uses - 1) & 1) && clock64() - t0 < (1ll << 31)) {
         }
       }
       if (clock64() - t0 >= (1ll << 31)) *abort_s = 1;
@@ -145,34 +173,53 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
     const int nt0 = wn * NTW, ntn = min(NTW, NTL - nt0);
     const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
     const double dt = p.dt;
+    uint64_t* gfull = bfull + grp * NSG;
+    uint64_t* gempty = bempty + grp * NSG;
+    const double* gst = stages + size_t(grp) * NSG * CF::STAGE;
     double en = 0.0;
-    uint32_t j = 0;
+    uint32_t j = 0;  // index into this group's ring
     bool dead = false;
     long long it = 0;
     for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
+      if (int(it % NG) != grp) continue;  // another group's item (its own ring)
       const int e = int(item / ntile), tile = int(item % ntile);
       const int s0 = tile * ST;
       const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
-      if (int(it % NG) != grp) {  // another group's item: its stages, in producer order
-        j += uint32_t(nb);
-        continue;
+      // u^{k-1} of this warp's outputs, requested now and used by the
+      // epilogue: the loads overlap the products. u^k comes from the
+      // diagonal block's state stage (the element's own tile) when the row
+      // starts with its diagonal block, else from global memory.
+      double2 upv[MTW][NTW], uk[MTW][NTW];
+#pragma unroll
+      for (int mt = 0; mt < MTW; ++mt) {
+        if constexpr (EPI == 0) break;
+        const int sh = s0 + (wm * MTW + mt) * 8 + gs;
+        const size_t me = (size_t(e) * S + (sh < S ? sh : 0)) * R;
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) {
+          const int r0 = (nt0 + q) * 8 + 2 * tg;
+          const bool valid = sh < S && q < ntn && r0 < R;
+          upv[mt][q] = (valid && p.uprev) ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
+          uk[mt][q] = make_double2(0.0, 0.0);
+        }
       }
+      const bool diag_first = EPI != 0 && p.col[rb] == e;
       double acc[MTW][NTW][2];
 #pragma unroll
       for (int mt = 0; mt < MTW; ++mt)
 #pragma unroll
         for (int q = 0; q < NTW; ++q) acc[mt][q][0] = acc[mt][q][1] = 0.0;
       for (int b = 0; b < nb; ++b) {
-        const int s = int(j % NST);
-        const uint32_t n = j / NST;
+        const int s = int(j % NSG);
+        const uint32_t n = j / NSG;
         ++j;
         if (dead) continue;
-        const bool okw = fx_wait(smem_u32(&bfull[s]), n & 1, abort_s);
+        const bool okw = fx_wait(smem_u32(&gfull[s]), n & 1, abort_s);
         if (__any_sync(0xffffffffu, !okw)) {
           dead = true;
           continue;
         }
-        const double* B = stages + size_t(s) * CF::STAGE;
+        const double* B = gst + size_t(s) * CF::STAGE;
         const double* X = B + CF::BSZ + (wm * MTW * 8 + gs) * R + tg;
         const double* Bt = B + tg * KP + nt0 * 8 + g;
 #pragma unroll
@@ -188,8 +235,19 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
             for (int q = 0; q < NTW; ++q)
               if (NTL % CF::WN == 0 || q < ntn) dmma_m8n8k4(acc[mt][q][0], acc[mt][q][1], a[mt], bb[q]);
         }
+        if (b == 0 && diag_first) {
+          const double* Xs = B + CF::BSZ;
+#pragma unroll
+          for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+            for (int q = 0; q < NTW; ++q) {
+              const int r0 = (nt0 + q) * 8 + 2 * tg;
+              if (q < ntn && r0 < R)
+                uk[mt][q] = *reinterpret_cast<const double2*>(Xs + ((wm * MTW + mt) * 8 + gs) * R + r0);
+            }
+        }
         __syncwarp();
-        if (lane == 0) fx_mbar_arrive(smem_u32(&bempty[s]));
+        if (lane == 0) fx_mbar_arrive(smem_u32(&gempty[s]));
       }
       // ---- epilogue (leap-frog, source, energy terms) ----
       if (!dead) {
@@ -209,10 +267,11 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
           for (int q = 0; q < NTW; ++q) {
             const int r0 = (nt0 + q) * 8 + 2 * tg;
             if (q >= ntn || r0 >= R) continue;  // rows come in pairs (R is even)
-            const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
+            const double2 uu = diag_first ? uk[mt][q] : __ldg(reinterpret_cast<const double2*>(p.x + me + r0));
             const double2 up =
-                p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0);
-            const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
+                EPI != 0 ? upv[mt][q]
+                         : (p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me + r0) : make_double2(0.0, 0.0));
+            const double u[2] = {uu.x, uu.y}, upr[2] = {up.x, up.y};
             double un[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -220,14 +279,15 @@ __global__ void __launch_bounds__(D64WCfg<R, NST, NG, WM, WN>::NT, MINB)
               const int cmp = r / NP, ii = r - cmp * NP;
               const double f = is_src ? Fk[cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
               const double y = acc[mt][q][h];
-              if (p.mode == kModeStep) un[h] = (2 * u[h] - upv[h]) + mi * ((-dt * dt) * (y - f));
-              else un[h] = (u[h] + dt * upv[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+              if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
+              else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
               if (p.energy != nullptr) {
                 const double d = un[h] - u[h];
                 en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
               }
             }
             *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+            note_nonfinite(p, un[0], un[1]);
           }
         }
       }
