@@ -15,8 +15,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
+# Benchmark-size goldens (several shots, subsampled receiver traces): a
+# schema of their own, used by tests/test_gpu_scale_parity.py.
+SCALE_GOLDENS = ("g_config1_full", "g_config3_sample")
+
+
 def golden_cases():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+                  if n not in SCALE_GOLDENS)
 
 
 def load_golden(name):

@@ -5,7 +5,9 @@ oracle/Makefile against the project's Eigen-subset shim
 (oracle/_ref/tsp_ref_run), on small seeded meshes, and stores inputs and
 outputs as .npz. Rebuild with:
 
-    make -C oracle REF=/root/reference && python tests/golden/make_golden.py [case ...]
+    make -C oracle && python tests/golden/make_golden.py [case ...]
+
+(the reference sources are read from $TSPEED_REF, default /root/reference).
 
 Cases named g_ba_* use the reference's BoundaryAdapted space
 (FESpace<N, Dunavant<2N>, BoundaryAdapted<N>>, Examples/src/Lamb.cpp:26).
@@ -128,14 +130,99 @@ def run_case(name, c, tmp):
     print(name, "ne", ne, "Np", Np, "steps", c["nsteps"], "last_time", info["last_time"])
 
 
+# Benchmark-size cases: the reference's stepping loop (TimeAdvance.cpp:41-59,
+# driven as Examples/src/Wedge.cpp:72-81 does) over a benchmark configuration's
+# full step count, one reference process per shot.
+#   g_config1_full: configuration 1 in full (40x20 squares -> 1,600 triangles,
+#     N=4, homogeneous, Ricker 8 Hz at (2000, 1500), 8 surface receivers,
+#     2,000 steps); every receiver sample and the final displacement.
+#   g_config3_sample: the 64-shot configuration's shape on its x0.2 sample
+#     (40x20 squares, N=5, log-normal vp, 128 surface receivers, 3,000 steps),
+#     8 seeded shots; receiver samples every SEIS_EVERY-th step (the 10 Hz
+#     Ricker's band lies far below the sampling rate), the final displacement
+#     of shots U_SHOTS.
+# dt = 0.4 x the CFL limit 2/sqrt(lmax(M^-1 B)), lmax by power iteration on the
+# oracle's operator, rounded to 3 significant digits.
+SCALE_CASES = {
+    "g_config1_full": dict(config=1, scale=1.0, nshots=1, seis_every=1, u_shots=(0,)),
+    "g_config3_sample": dict(config=3, scale=0.2, nshots=8, shot_seed=2024, seis_every=30, u_shots=(0, 5)),
+}
+
+
+def oracle_lmax(prob, iters=200):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import tsp_oracle as O
+    tri = prob.mesh.tri.astype(np.int64)
+    sp = O.make_space(prob.N)
+    geo = O.geometry(prob.mesh.xy, tri)
+    nb, ned = O.neighbours(tri)
+    rp, cols, blocks, minv = O.assemble(sp, geo, nb, ned, prob.lam, prob.mu, prob.rho, prob.penalty)
+    ne, Np = prob.mesh.ne, prob.Np
+    mi = np.concatenate([np.repeat(minv, Np), np.repeat(minv, Np)])
+    x = np.random.default_rng(0).standard_normal(2 * ne * Np)
+    lam = 0.0
+    for _ in range(iters):
+        y = mi * O.apply_B(rp, cols, blocks, x, ne, Np)
+        lam = float(x @ y / (x @ x))
+        x = y / np.linalg.norm(y)
+    return lam
+
+
+def run_scale_case(name, c, tmp):
+    from concurrent.futures import ThreadPoolExecutor
+    kw = dict(scale=c["scale"])
+    if c["config"] == 3:
+        kw.update(nshots=c["nshots"], shot_seed=c["shot_seed"])
+    prob = W.config(c["config"], **kw)
+    m = prob.mesh
+    lmax = oracle_lmax(prob)
+    dt = float(f"{0.4 * 2.0 / np.sqrt(lmax):.3g}")
+    msh, rcvf, matf = (os.path.join(tmp, name + s) for s in (".msh", ".rcv", ".mat"))
+    W.write_gmsh(msh, m)
+    W.write_rcv(rcvf, prob.receivers)
+    np.stack([prob.lam, prob.mu, prob.rho], 1).astype(np.float64).tofile(matf)
+    nsteps = prob.nsteps
+
+    def one(k):
+        sr = prob.sources[k]
+        out = os.path.join(tmp, f"{name}.{k}")
+        cmd = [REF, "--mesh", msh, "--N", str(prob.N), "--mat", matf, "--rcv", rcvf, "--out", out, "--dt", repr(dt),
+               "--nsteps", str(nsteps), "--src", repr(sr.x), repr(sr.y), "--ricker", repr(sr.f0), repr(sr.t0),
+               repr(sr.amp), "--sdir", str(sr.direction), "--penalty", repr(prob.penalty)]
+        info = json.loads(subprocess.run(cmd, check=True, capture_output=True, text=True).stdout)
+        seis = np.fromfile(out + ".seis.bin", dtype=np.float64).reshape(nsteps, len(prob.receivers), 2)
+        u = open(out + ".u.bin", "rb").read()
+        rec = 8 + 16 * m.ne * prob.Np
+        snaps = {int(np.frombuffer(u, np.int64, 1, i)[0]): np.frombuffer(u, np.float64, 2 * m.ne * prob.Np, i + 8)
+                 for i in range(0, len(u), rec)}
+        return info, seis[::c["seis_every"]].copy(), snaps[nsteps].copy()
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        res = list(ex.map(one, range(prob.nshots)))
+    d = dict(xy=m.xy, tri=m.tri, region=m.region, lam=prob.lam, mu=prob.mu, rho=prob.rho, N=prob.N,
+             penalty=prob.penalty, dt=dt, lmax_oracle=lmax, nsteps=nsteps,
+             src=np.array([(sr.x, sr.y) for sr in prob.sources]),
+             ricker=np.array([(sr.f0, sr.t0, sr.amp, sr.direction) for sr in prob.sources]),
+             rcv=np.array(prob.receivers), seis_every=c["seis_every"],
+             seis=np.stack([r[1] for r in res]), u_shots=np.array(c["u_shots"]),
+             u_final=np.stack([res[k][2] for k in c["u_shots"]]),
+             last_time=res[0][0]["last_time"], ref_loop_s=np.array([r[0]["loop_s"] for r in res]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
+    print(name, "ne", m.ne, "Np", prob.Np, "shots", prob.nshots, "steps", nsteps, "dt", dt,
+          "loop_s", [round(r[0]["loop_s"], 1) for r in res])
+
+
 def main():
     if not os.path.exists(REF):
-        sys.exit(f"{REF} missing: run `make -C oracle REF=/root/reference` first")
+        sys.exit(f"{REF} missing: run `make -C oracle` first (reference sources from $TSPEED_REF)")
     only = sys.argv[1:]
     with tempfile.TemporaryDirectory() as tmp:
         for name, c in CASES.items():
             if not only or name in only:
                 run_case(name, c, tmp)
+        for name, c in SCALE_CASES.items():
+            if not only or name in only:
+                run_scale_case(name, c, tmp)
 
 
 if __name__ == "__main__":
