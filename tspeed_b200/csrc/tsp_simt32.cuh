@@ -1,0 +1,308 @@
+// Batched step with an FP32 operator on the CUDA cores, warp-specialised and
+// persistent (internal header of tspeed_b200).
+//
+// Per work item (element row e, tile of 64 shots) the block SpMM
+//   Y[shot][r] = sum_b sum_k X_{col b}[shot][k] B_b[r][k]
+// runs in FP32 (FP32 operator blocks, the FP32 shadow of the state, FP32
+// accumulation) with register tiles large enough that the FP32 pipe, not the
+// shared-memory or issue bandwidth, bounds the products: each lane owns
+// 8 shots x RL rows (RL = 6 at 2Np = 42: 48 accumulators fed by two 16-byte
+// loads of the state and RL/2 8-byte loads of the block per K step). The
+// leap-frog update, the source, the receivers and the energy terms stay in
+// FP64 (u^k, u^{k-1} and u^{k+1} in FP64); the epilogue also writes the FP32
+// shadow of u^{k+1} that the next step's neighbours read.
+//
+// Data flow: one producer lane per consumer group streams, per block, two
+// bulk copies into the group's own ring of NSG stages (cp.async.bulk,
+// completion on mbarriers, no multicast): the stored FP32 block (column-major,
+// pitch KP = 2Np padded to 4) and the neighbour's FP32 shadow tile (2Np rows
+// of 64 shots, contiguous). A ring per group makes every mbarrier wait
+// unambiguous (index j - NSG of a ring is always its own group's consumed
+// block). NGR groups of NWG warps take the CTA's items in turn, so one
+// group's epilogue (FP64 global loads and stores) overlaps the others'
+// products.
+//
+// Lane (sg, rg) of warp w of a group: shots 4 sg .. 4 sg + 3 and
+// 32 + 4 sg .. 32 + 4 sg + 3 (each quarter-warp reads 128 contiguous bytes
+// of a state row: conflict-free), rows w RW + rg RL .. + RL - 1 with
+// RW = 4 RL. Rows at or beyond 2Np (the last warp's padding) are computed
+// from in-bounds shared memory (the stage's tail) and never stored.
+//
+// Every wait is bounded (about a second); on a timeout the CTA raises an
+// abort flag in shared memory, every role stops waiting, the consumer warps
+// keep their named barriers balanced, the producers wait (bounded) for their
+// copies in flight, and err_flag tells the host that the results are void.
+#pragma once
+
+#include <stdint.h>
+
+#include "tsp_kernels.cuh"
+#include "tsp_tcfx.cuh"
+#include "tsp_tcgen05.cuh"
+
+namespace tsp {
+
+template <int R>
+struct S32WCfg {
+  static constexpr int KP = (R + 3) & ~3;  // stored block pitch of batched handles
+  static constexpr int ST = 64;            // shots per tile (the FP32 shadow's tile)
+  // Rows per lane (even: the FP64 epilogue works on row pairs): padding
+  // rows kept small with at most two warps per item.
+  static constexpr int RL = R <= 8 ? 2 : R <= 16 ? 4 : R <= 24 ? 6 : R <= 32 ? 4 : R <= 48 ? 6 : 8;
+  static constexpr int RW = 4 * RL;                   // rows per warp
+  static constexpr int NWG = (R + RW - 1) / RW;       // warps per group
+  static constexpr int BSZ = R * KP;                  // floats: operator stage [k][r], pitch KP
+  static constexpr int XSZ = R * ST;                  // floats: state stage [k][shot]
+  static constexpr int STAGE = BSZ + XSZ;
+  static_assert((BSZ * 4) % 16 == 0 && (STAGE * 4) % 16 == 0, "16-byte aligned stages");
+  // The last warp's padding rows read at most this far into a stage.
+  static_assert((R - 1) * KP + NWG * RW <= STAGE, "padding rows stay inside the stage");
+};
+
+template <int R, int NGR, int NSG>
+struct S32WLayout {
+  typedef S32WCfg<R> C;
+  static constexpr int NT = (NGR * C::NWG + 1) * 32;
+  static constexpr int NST = NGR * NSG;
+  static constexpr size_t smem_bytes() {
+    return size_t(NST) * C::STAGE * sizeof(float) + size_t(2 * NST) * sizeof(uint64_t) + 16;
+  }
+};
+
+// Groups x stages per group that fit in shared memory.
+template <int R, int NGR>
+constexpr int s32w_fit_nsg() {
+  constexpr size_t one = S32WLayout<R, NGR, 1>::smem_bytes();
+  constexpr size_t budget = 227 * 1024;
+  return int(budget / one) >= 6 ? 6 : int(budget / one);
+}
+
+template <int R, int NGR, int NSG>
+__global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
+    k_step_batched32w(const StepParams p, int* err_flag) {
+  typedef S32WCfg<R> CF;
+  typedef S32WLayout<R, NGR, NSG> LY;
+  constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, RL = CF::RL, RW = CF::RW, NWG = CF::NWG;
+  constexpr int NST = LY::NST;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* stages = reinterpret_cast<float*>(smem_raw);
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NGR][NSG] stage landed
+  uint64_t* bempty = bfull + NST;                                                    // [NGR][NSG] stage consumed
+  volatile int* abort_s = reinterpret_cast<volatile int*>(bempty + NST);
+
+  if (*reinterpret_cast<volatile int*>(err_flag) != 0) return;  // an earlier launch of the run timed out
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (t == 0) {
+    *abort_s = 0;
+    for (int i = 0; i < NST; ++i) {
+      fx_mbar_init(smem_u32(&bfull[i]), 1);
+      fx_mbar_init(smem_u32(&bempty[i]), NWG);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = t; i < NST * CF::STAGE; i += LY::NT) stages[i] = 0.0f;
+  __syncthreads();
+
+  const int S = p.S;
+  const int ntile = (S + ST - 1) / ST;
+  const long long nitems = (long long)p.ne * ntile;
+  const long long G = gridDim.x;
+  const float* blocks = reinterpret_cast<const float*>(p.blocks);
+
+  if (warp == NGR * NWG) {
+    // ---------------- producers: lane g fills ring g ----------------
+    if (lane < NGR) {
+      const int g = lane;
+      uint64_t* gfull = bfull + g * NSG;
+      uint64_t* gempty = bempty + g * NSG;
+      float* gst = stages + size_t(g) * NSG * CF::STAGE;
+      constexpr uint32_t bbytes = uint32_t(R) * KP * 4, xbytes = uint32_t(R) * ST * 4;
+      uint32_t j = 0;
+      bool ok = true;
+      for (long long item = blockIdx.x + g * G; item < nitems && ok; item += NGR * G) {
+        const int e = int(item / ntile), tile = int(item % ntile);
+        const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+        for (int b = 0; b < nb; ++b) {
+          const int s = int(j % NSG);
+          const uint32_t n = j / NSG;
+          if (n > 0 && !fx_wait(smem_u32(&gempty[s]), (n - 1) & 1, abort_s)) {
+            ok = false;
+            break;
+          }
+          const int c = p.col[rb + b];
+          const uint32_t bar = smem_u32(&gfull[s]);
+          const uint32_t dB = smem_u32(gst + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 4;
+          fx_mbar_arrive_tx(bar, bbytes + xbytes);
+          fx_bulk_g2s(dB, blocks + size_t(rb + b) * R * KP, bbytes, bar);
+          fx_bulk_g2s(dX, p.x32_in + (size_t(c) * ntile + tile) * R * ST, xbytes, bar);
+          ++j;
+        }
+      }
+      // Every issued copy lands before the CTA ends (bounded; copies
+      // complete). At most one use of a stage is in flight.
+      const long long t0 = clock64();
+      for (int s = 0; s < NSG; ++s) {
+        if (j <= uint32_t(s)) continue;
+        const uint32_t uses = (j - 1 - s) / NSG + 1;
+        while (!mbar_try(smem_u32(&gfull[s]), (uses - 1) & 1) && clock64() - t0 < (1ll << 31)) {
+        }
+      }
+      if (clock64() - t0 >= (1ll << 31)) *abort_s = 1;
+    }
+  } else {
+    // ---------------- consumers ----------------
+    const int grp = warp / NWG, w = warp % NWG, tl = t - grp * NWG * 32;
+    const int sg = lane & 7, rg = lane >> 3;
+    const int rbase = w * RW + rg * RL;  // the lane's first row
+    const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+    const double dt = p.dt;
+    uint64_t* gfull = bfull + grp * NSG;
+    uint64_t* gempty = bempty + grp * NSG;
+    const float* gst = stages + size_t(grp) * NSG * CF::STAGE;
+    double en = 0.0;
+    uint32_t j = 0;  // index into this group's ring
+    bool dead = false;
+    long long it = 0;
+    for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
+      if (int(it % NGR) != grp) continue;  // another group's item (its own ring)
+      const int e = int(item / ntile), tile = int(item % ntile);
+      const int s0 = tile * ST;
+      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      float acc[RL][8];
+#pragma unroll
+      for (int i = 0; i < RL; ++i)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[i][q] = 0.0f;
+      for (int b = 0; b < nb; ++b) {
+        const int s = int(j % NSG);
+        const uint32_t n = j / NSG;
+        ++j;
+        if (dead) continue;
+        const bool okw = fx_wait(smem_u32(&gfull[s]), n & 1, abort_s);
+        if (__any_sync(0xffffffffu, !okw)) {
+          dead = true;
+          continue;
+        }
+        const float* Bs = gst + size_t(s) * CF::STAGE + rbase;
+        const float* Xs = gst + size_t(s) * CF::STAGE + CF::BSZ + 4 * sg;
+#pragma unroll 2
+        for (int kk = 0; kk < R; ++kk) {
+          const float4 xa = *reinterpret_cast<const float4*>(Xs + kk * ST);
+          const float4 xb = *reinterpret_cast<const float4*>(Xs + kk * ST + 32);
+          const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+          float bv[RL];
+#pragma unroll
+          for (int i = 0; i < RL; i += 2) {
+            const float2 b2 = *reinterpret_cast<const float2*>(Bs + kk * KP + i);
+            bv[i] = b2.x;
+            bv[i + 1] = b2.y;
+          }
+#pragma unroll
+          for (int i = 0; i < RL; ++i)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc[i][q] = fmaf(xv[q], bv[i], acc[i][q]);
+        }
+        __syncwarp();
+        if (lane == 0) fx_mbar_arrive(smem_u32(&gempty[s]));
+      }
+      // ---- epilogue (FP64 leap-frog, source, energy; FP32 shadow) ----
+      const size_t tix = size_t(e) * ntile + tile;
+      if (!dead) {
+        const double mi = p.minv[e];
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          // Shots 32 half + 4 sg + q, q < 4; their source terms first.
+          bool src[4];
+          double Fk[4][2];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int sh = s0 + 32 * half + 4 * sg + q;
+            src[q] = sh < S && (p.src_elem[sh] == e) && (k < p.nF);
+            Fk[q][0] = src[q] ? p.F[(size_t(sh) * p.nF + k) * 2] : 0.0;
+            Fk[q][1] = src[q] ? p.F[(size_t(sh) * p.nF + k) * 2 + 1] : 0.0;
+          }
+          float sv[RL][4];
+#pragma unroll
+          for (int i = 0; i < RL / 2; ++i) {
+            // Row pair rbase + 2i of the four shots: both levels' loads first.
+            const int r0 = rbase + 2 * i;
+            double2 uu[4], up[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int sh = s0 + 32 * half + 4 * sg + q;
+              const bool v = sh < S && r0 < R;
+              const size_t me = (size_t(e) * S + (v ? sh : 0)) * R + (v ? r0 : 0);
+              uu[q] = v ? __ldg(reinterpret_cast<const double2*>(p.x + me)) : make_double2(0.0, 0.0);
+              up[q] = (v && p.uprev) ? *reinterpret_cast<const double2*>(p.uprev + me) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int sh = s0 + 32 * half + 4 * sg + q;
+              const bool v = sh < S && r0 < R;
+              const double u[2] = {uu[q].x, uu[q].y}, upr[2] = {up[q].x, up[q].y};
+              double un[2];
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int r = r0 + h;
+                const int cmp = r / NP, ii = r - cmp * NP;
+                const double f = (src[q] && r < R) ? Fk[q][cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+                const double y = double(acc[2 * i + h][4 * half + q]);
+                if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
+                else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+                if (p.energy != nullptr && v) {
+                  const double d = un[h] - u[h];
+                  en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+                }
+                sv[2 * i + h][q] = v ? float(un[h]) : 0.0f;
+              }
+              if (v) {
+                *reinterpret_cast<double2*>(p.out + (size_t(e) * S + sh) * R + r0) = make_double2(un[0], un[1]);
+                note_nonfinite(p, un[0], un[1]);
+              }
+            }
+          }
+          // FP32 shadow of u^{k+1}: row r, shots 32 half + 4 sg .. + 3 (one
+          // 16-byte store; the 8 lanes of a row group write 128 bytes).
+#pragma unroll
+          for (int i = 0; i < RL; ++i) {
+            const int r = rbase + i;
+            if (r < R)
+              *reinterpret_cast<float4*>(p.x32_out + (tix * R + r) * ST + 32 * half + 4 * sg) =
+                  make_float4(sv[i][0], sv[i][1], sv[i][2], sv[i][3]);
+          }
+        }
+      }
+      // ---- receivers (the condition is the same for every warp of the group) ----
+      if (p.rcv_ptr != nullptr) {
+        const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+        if (q1 > q0) {
+          // u^{k+1} of this item is visible to the whole group (barrier 1 + grp).
+          asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(NWG * 32) : "memory");
+          if (!dead) {
+            const long long slot = k % p.seis_cap;
+            const int nwork = (q1 - q0) * ST * 2;
+            for (int wk = tl; wk < nwork; wk += NWG * 32) {
+              const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
+              const int sh = s0 + sl;
+              if (sh >= S) continue;
+              const int rid = p.rcv_id[q];
+              const double* ph = p.rcv_phi + size_t(rid) * NP;
+              const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
+              double v = 0.0;
+              for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+              p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+            }
+          }
+        }
+      }
+    }
+    if (p.energy != nullptr) {
+      const double v = warp_sum(en);
+      if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
+    }
+  }
+  __syncthreads();
+  if (t == 0 && *abort_s) atomicExch(err_flag, 1);
+}
+
+}  // namespace tsp
