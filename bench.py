@@ -152,9 +152,12 @@ def estimate_dt(sim, cfl_fraction=0.4, iters=60):
     return cfl_fraction * 2.0 / math.sqrt(lmax), lmax
 
 
-# The FP64 batched step kernel at 2Np = 42 (64-shot tiles, 5-stage ring, two
-# consumer groups, 8 x 1 warps per group).
-D64_KERNEL = "k_step_batched64w<42,5,2,1,8,1>"
+# FP64 batched step kernels at 2Np = 42 by variant (tsp_get_kernel_variant):
+# 5 warp-specialised DMMA, two consumer groups of 8 warps with a 3-stage ring
+# each; 6 the same kernel with one group of 16 warps and a 6-stage ring; 3 the
+# single-role DMMA kernel; 2 the CUDA-core kernel.
+D64_KERNELS = {5: "k_step_batched64w<42,3,2,1,8,1,0>", 6: "k_step_batched64w<42,6,1,1,8,2,1>",
+               3: "k_step_batched64d<42>", 2: "k_step_batched<42,double>"}
 
 # Nominal dense FP64 tensor-core rate of a B200 (DMMA); MEASURED_PEAKS.json
 # holds no FP64 figure.
@@ -195,11 +198,16 @@ def prepare(sim, prob, dt, nsteps):
         sim.set_ricker(k, s.f0, s.t0, s.amp, s.direction, nsteps)
 
 
-def cpu_reference_sample(nprocs=1, nsteps=300, scale=0.2, timeout=600):
+def cpu_reference_sample(nprocs=1, nsteps=20, scale=0.5, timeout=900):
     """The reference's own CPU path (oracle/_ref, compiled from its sources)
     on a bounded sample of the workload: the same configuration shrunk to
-    `scale` per axis, one shot per process, `nprocs` processes in parallel
-    (the reference is single-threaded). Returns (DOF-steps/s, sample text)."""
+    `scale` per axis (x0.5: 10,000 triangles, whose operator, like the full
+    configuration's, is far larger than the host caches: the per-DOF rate
+    matches the full 40,000-triangle mesh's, while a x0.2 sample fits in cache
+    and runs 1.5x faster), one shot per process, `nprocs` processes in
+    parallel (the reference is single-threaded), `nsteps` steps each; the
+    reference's set-up (O(ne^2) neighbour search, assembly) is not timed.
+    Returns (DOF-steps/s, sample text)."""
     if not os.path.exists(REF_BIN):
         return None, "reference binary missing"
     p = W.config(3, scale=scale, nshots=max(1, nprocs))
@@ -229,18 +237,112 @@ def cpu_reference_sample(nprocs=1, nsteps=300, scale=0.2, timeout=600):
     return value, sample
 
 
+GOLDEN_C3 = os.path.join(ROOT, "tests", "golden", "g_config3_sample.npz")
+
+
+def run_on_golden(g, precision, shots, variant=None):
+    """Runs a golden problem (committed fixture) with the given shots
+    (indices into its sources); returns the seismograms sampled like the
+    golden's, [S][nsteps / every][nr][2]."""
+    old = os.environ.get("TSP_BATCHED_VARIANT")
+    if variant is None:
+        os.environ.pop("TSP_BATCHED_VARIANT", None)
+    else:
+        os.environ["TSP_BATCHED_VARIANT"] = str(variant)
+    try:
+        n = int(g["nsteps"])
+        with capi.Simulation.create(g["xy"], g["tri"], int(g["N"]), g["lam"], g["mu"], g["rho"],
+                                    [tuple(g["src"][k]) for k in shots], g["rcv"], penalty=float(g["penalty"]),
+                                    precision=precision) as s:
+            v = s.kernel_variant
+            s.set_dt(float(g["dt"]))
+            for i, k in enumerate(shots):
+                f0, t0, amp, sdir = g["ricker"][k]
+                s.set_ricker(i, f0, t0, amp, int(sdir), n)
+            s.set_seismogram_capacity(n)
+            s.first_step()
+            s.run(n - 1)
+            return s.seismograms(0, n)[:, ::int(g["seis_every"])], v
+    finally:
+        if old is None:
+            os.environ.pop("TSP_BATCHED_VARIANT", None)
+        else:
+            os.environ["TSP_BATCHED_VARIANT"] = old
+
+
+def errors_vs_reference():
+    """Seismogram relative L2 error of each form against the reference's own
+    FP64 run of the 64-shot configuration's shape on its x0.2 sample
+    (tests/golden/g_config3_sample.npz: 1,600 triangles, N=5, log-normal vp,
+    8 shots, 3,000 steps, 128 receivers; made by the reference's stepping
+    loop compiled from its sources)."""
+    if not os.path.exists(GOLDEN_C3):
+        return None
+    g = np.load(GOLDEN_C3)
+    ns = len(g["src"])
+    ref = g["seis"]
+    out = {"golden": "tests/golden/g_config3_sample.npz", "shots": ns, "steps": int(g["nsteps"]),
+           "receivers": int(len(g["rcv"])), "forms": {}}
+
+    def err(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    for name, prec, var in (("batched_fp64", "fp64", None), ("batched_fp32_operator", "fp32", None),
+                            ("batched_fp32_cuda_core", "fp32", 0)):
+        seis, v = run_on_golden(g, prec, list(range(ns)), var)
+        out["forms"][name] = {"err": err(seis, ref), "kernel_variant": v}
+    errs = []
+    for k in (0, ns - 1):
+        seis, _ = run_on_golden(g, "fp64", [k])
+        errs.append(err(seis[0], ref[k]))
+    out["forms"]["plain_fp64_single_shot"] = {"err": max(errs), "shots_checked": [0, ns - 1]}
+    return out
+
+
+def energy_drift(prob, dt, nsteps=500):
+    """Discrete-energy drift max_k |E^k - E^0| / E^0 of each timed form, with
+    the sources off and a seeded initial field per shot (a Gaussian pulse of
+    the vertical displacement, 150 m wide, at the shot's source point,
+    projected on the device), over nsteps steps of the configuration's mesh."""
+    pts = capi.quadrature_points(prob.N, prob.mesh.xy, prob.mesh.tri)
+    out = {"steps": nsteps, "initial_field": "Gaussian pulse of u_y (sigma 150 m) at each source point",
+           "forms": {}}
+    for name, prec, nsh in (("batched_fp64", "fp64", prob.nshots), ("batched_fp32_operator", "fp32", prob.nshots),
+                            ("plain_fp64_single_shot", "fp64", 1)):
+        with capi.Simulation.create(prob.mesh.xy, prob.mesh.tri, prob.N, prob.lam, prob.mu, prob.rho,
+                                    [(sr.x, sr.y) for sr in prob.sources[:nsh]], [], penalty=prob.penalty,
+                                    precision=prec) as s:
+            s.set_dt(dt)
+            for k in range(nsh):
+                sr = prob.sources[k]
+                r2 = (pts[..., 0] - sr.x) ** 2 + (pts[..., 1] - sr.y) ** 2
+                vals = np.zeros(pts.shape)
+                vals[..., 1] = 1e-3 * np.exp(-r2 / (2 * 150.0 ** 2))
+                s.set_initial_values(k, vals, None)
+            s.enable_energy(True)
+            s.first_step()
+            s.run(nsteps - 1)
+            E = s.energy(0, nsteps)
+            v = s.kernel_variant
+        out["forms"][name] = {"drift": float(np.max(np.abs(E - E[0])) / E[0]), "kernel_variant": v}
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    ncores = os.cpu_count() or 1
+    # One single-threaded reference process per host core, capped so that
+    # the processes' operators (1.4 GB each at the x0.5 sample) stay well
+    # inside host memory.
+    ncores = min(os.cpu_count() or 1, 32)
     nsteps = max(10, args.steps)
-    v, sample = cpu_reference_sample(nprocs=ncores, nsteps=nsteps)
+    v, sample = cpu_reference_sample(nprocs=ncores, nsteps=nsteps, scale=args.ref_scale)
     cfg = config_dict(args, None)
     if v is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+    line = {"impl": "reference", "sample": sample, "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "reference", "sample": sample},
@@ -362,6 +464,8 @@ def main():
     ap.add_argument("--nshots", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
+    ap.add_argument("--ref-scale", type=float, default=0.5,
+                    help="per-axis scale of the sample the reference's CPU path runs (--impl reference)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-FP64, accuracy, e2e and CPU legs")
     ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config4", "config5"],
                     help="config3: the 64-shot headline; config2/config5: single-shot forms side by side")
@@ -392,6 +496,7 @@ def main():
     K, Wm = args.steps, max(3, args.warmup)
     sim = capi.Simulation.from_problem(prob, precision=args.precision, device=local_rank)
     variant = sim.kernel_variant if (prob.nshots > 1 and args.precision == "fp32") else None
+    variant64 = sim.kernel_variant if (prob.nshots > 1 and args.precision == "fp64") else None
     dt, lmax = estimate_dt(sim)
     prepare(sim, prob, dt, K + Wm + 2)
     sim.set_seismogram_capacity(K + Wm + 2)
@@ -419,7 +524,7 @@ def main():
     achieved = algo / (ms_step / 1e3) / 1e9
     kernel = (KERNELS.get(variant, "batched") if variant is not None else
               "k_step_rows<42>" if prob.nshots == 1 else
-              D64_KERNEL if args.precision == "fp64" else "k_step_batched<42>")
+              D64_KERNELS.get(variant64, "batched") if args.precision == "fp64" else "k_step_batched<42>")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("bf16x3 fixed-point operator, f64 state" if form == "fx" else
@@ -440,6 +545,7 @@ def main():
         # The FP64 batched step is bound by the FP64 tensor cores (DMMA), not HBM.
         line["roofline_hbm"] = line["roofline"]
         line["roofline"] = fp64_tensor_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel, local_rank)
+        line["roofline"]["kernel_variant"] = variant64
         tr = captured_traffic(kernel, prob.mesh.ne, prob.nshots) if prob.N == 5 else None
         line["roofline"]["traffic"] = tr
         line["roofline"]["traffic_unit"] = "bytes per launch (ncu, profiles/traffic.json, scaled by element rows)"
@@ -477,6 +583,7 @@ def main():
         # Exact FP64 for all shots: the FP64 tensor-core batched step.
         if prob.nshots > 1 and args.precision != "fp64":
             with capi.Simulation.from_problem(prob, precision="fp64") as s64:
+                v64var = s64.kernel_variant
                 prepare(s64, prob, dt, K + Wm + 2)
                 s64.first_step()
                 s64.run(Wm)
@@ -487,7 +594,7 @@ def main():
             line["batched_fp64"] = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / K,
                                     "speedup_vs_plain_fp64": v64 / v1, "seismogram_err": "exact FP64",
                                     "roofline": fp64_tensor_roofline(nnzb64, prob.Np, prob.nshots, ms64 / K,
-                                                                     D64_KERNEL)}
+                                                                     D64_KERNELS.get(v64var, "batched"))}
         # Accuracy of the measured form over the full step count against FP64
         # computed by the CUDA-core FP64 kernel (TSP_BATCHED_VARIANT=2): for the
         # FP64 tensor-core form this is the difference of two FP64 summation
@@ -521,6 +628,13 @@ def main():
             line["accuracy_steps"] = nacc
             if "batched_fp32_operator" in line:
                 line["batched_fp32_operator"]["seismogram_rel_l2_err_vs_fp64"] = errs["fp32"]
+        # The forms against the reference itself (committed golden of the
+        # reference's own run), and their discrete-energy drift.
+        vs_ref = errors_vs_reference()
+        if vs_ref is not None:
+            line["seismogram_rel_l2_err_vs_reference"] = vs_ref
+        if prob.nshots > 1:
+            line["energy_drift"] = energy_drift(prob, dt)
         # End to end through the public C-ABI with host buffers.
         ne_steps = K
         t0 = time.perf_counter()
@@ -540,7 +654,7 @@ def main():
                        "includes": "tsp_create (mesh upload, device assembly, point location, kernel choice), "
                                    "force tables, first_step + run, read-back of every step's receiver samples "
                                    "(the shot gathers)"}
-        v_cpu, sample = cpu_reference_sample(nprocs=1, nsteps=200)
+        v_cpu, sample = cpu_reference_sample(nprocs=1, nsteps=10)
         line["cpu_baseline"] = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample}
     if rank == 0:
         print(json.dumps(line))

@@ -22,8 +22,10 @@
  *     FESpace_imp.hpp:152-153). On the device the library keeps an
  *     element-major, shot-interleaved layout.
  *   - tsp_first_step, tsp_step and tsp_run allocate no device memory;
- *     tsp_run instantiates a CUDA graph the first time it sees a step count
- *     (per parity of the current level) and replays it afterwards.
+ *     tsp_run splits a run into pieces of 256 steps and the powers of two of
+ *     the remainder, each a CUDA graph instantiated the first time its length
+ *     (per parity of the current level) is met and replayed afterwards: at
+ *     most 18 graphs per handle, whatever step counts are asked for.
  */
 #ifndef TSPEED_B200_H
 #define TSPEED_B200_H 1
@@ -207,20 +209,29 @@ int tsp_first_step(tsp_handle* h);
 /* LeapFrog::step (TimeAdvance.cpp:41-59), once. */
 int tsp_step(tsp_handle* h);
 
-/* nsteps calls of LeapFrog::step, replayed from a cached CUDA graph. */
+/* nsteps calls of LeapFrog::step, replayed from cached CUDA graphs (pieces
+ * of at most 256 steps). Asynchronous: returns once the work is queued on the
+ * handle's stream. */
 int tsp_run(tsp_handle* h, int64_t nsteps);
 
 /* tsp_run with CUDA events recorded on the handle's stream around the graph
- * replay; synchronises and returns the device time in milliseconds. */
+ * replay; synchronises and returns the device time in milliseconds. Returns
+ * TSP_ERR_NONFINITE if any step since the initial values (or the resumed
+ * state) were set wrote a NaN or infinite displacement: every step kernel
+ * raises a device flag then (the reference has no such check; its Eigen loop
+ * carries NaNs on silently). */
 int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
 
-/* Kernel variant of the batched FP32 step chosen for this handle by the
- * autotuner at creation (or forced by TSP_BATCHED_VARIANT): 0 K-split /
- * pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel, 2 non-persistent
- * CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64 handles with
- * several shots: 5 warp-specialised FP64 tensor-core (DMMA) kernel (default),
- * 3 single-role DMMA kernel, 2 CUDA-core kernel (3 and 2 when forced). No
- * counterpart in the reference (its step is a single CPU path). */
+/* Kernel variant of the batched step chosen for this handle by the
+ * autotuner at creation (or forced by TSP_BATCHED_VARIANT). FP32 operator:
+ * 0 K-split / pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel,
+ * 2 non-persistent CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64
+ * operator with several shots: 5 warp-specialised FP64 tensor-core (DMMA)
+ * kernel with two consumer groups of 8 warps (8 shots x all rows per warp),
+ * 6 the same kernel with one group of 16 warps (8 shots x half the rows) and
+ * an epilogue without load latency, 3 single-role DMMA kernel, 2 CUDA-core
+ * kernel.
+ * No counterpart in the reference (its step is a single CPU path). */
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant);
 
 /* Number of leap-frog steps done (first_step counts as 1) and the
@@ -256,8 +267,9 @@ int tsp_get_energy(tsp_handle* h, int64_t k0, int64_t nk, double* out);
 int tsp_get_state(tsp_handle* h, double* u_prev, double* u_cur, int64_t* steps_done, double* last_time);
 int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int64_t steps_done, double last_time);
 
-/* Sets *bad to 1 if any displacement value of the current level is not
- * finite (NaN/Inf watchdog). */
+/* NaN/Inf watchdog: sets *bad to 1 if a step kernel has written a non-finite
+ * displacement since the initial values were set, or if any value of the
+ * current level is not finite. Synchronises the handle's stream. */
 int tsp_check_finite(tsp_handle* h, int32_t* bad);
 
 /* One product y = B x with the handle's operator (MyMatMultiDim::vecMult,
@@ -275,9 +287,12 @@ int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax);
  * iteration vectors and the accumulators live in a fixed 32 MiB file-scope
  * device array (4 Mi doubles) that every GPU loading the library holds until
  * exit, so 2*ne*2Np + 3 must not exceed 4,194,304 (TSP_ERR_ARG otherwise).
- * The first call on a device looks up that array's device address; make it
- * before any stream capture. All calls share the array: calls that overlap
- * on the GPU (several handles, threads or streams at once) race. Calls no
+ * Every call looks up that array's device address in the current context (a
+ * host query, so a context reset leaves no stale address behind); the first
+ * call on a device may load the library's device code, so make it before any
+ * stream capture. All calls share the array and each re-initialises it:
+ * calls that overlap on the GPU (several handles, threads or streams at once)
+ * race. Multi-mesh groups are rejected (TSP_ERR_UNSUPPORTED). Calls no
  * cudaMalloc/cudaFree. */
 int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* lmax);
 

@@ -29,6 +29,7 @@
 #ifndef TSPEED_GPU_HPP
 #define TSPEED_GPU_HPP 1
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <fstream>
@@ -287,19 +288,37 @@ class LeapFrog {
     check(tsp_set_initial(h_, 0, u0_.empty() ? nullptr : u0_.data(), v0_.empty() ? nullptr : v0_.data()), h_);
     check(tsp_first_step(h_), h_);
     last_time_ = dt_;
+    steps_ = 1;
+    pending_ = 0;
     completed_ = false;
     dirty_ = true;
   }
-  // LeapFrog::step (TimeAdvance.cpp:41-59).
+  // LeapFrog::step (TimeAdvance.cpp:41-59). The step is queued: steps run on
+  // the device as one graph-replayed tsp_run when something reads the state
+  // (u(), field_out, L2error, write_receivers, handle()), so a loop of
+  // step() calls costs what tsp_run does. The time and is_running() follow
+  // the reference's accumulation at once (TimeAdvance.cpp:46, 56-57).
   void step() {
-    check(tsp_step(h_), h_);
+    if (!h_) throw Error(TSP_ERR_STATE, "step before first_step");
+    ++pending_;
+    ++steps_;
     const double t = last_time_ + dt_;
     last_time_ = t;
     if (t >= tmax_ - dt_) completed_ = true;  // TimeAdvance.cpp:56-57
     dirty_ = true;
   }
   bool is_running() const { return !completed_; }
+  double last_time() const { return last_time_; }
+  // Runs the queued steps (errors of queued steps surface here).
+  void flush() {
+    if (pending_ > 0) {
+      const int64_t n = pending_;
+      pending_ = 0;
+      check(tsp_run(h_, n), h_);
+    }
+  }
   const std::vector<double>& u() {
+    flush();
     if (dirty_) {
       uh_.resize(2 * size_t(Xh_->ne()) * Xh_->nln());
       check(tsp_get_u(h_, 0, uh_.data()), h_);
@@ -310,8 +329,12 @@ class LeapFrog {
   const std::vector<double>& get_uh() { return u(); }
   // Xh->field_out(fname, u(), step) and Xh->L2error(uex, u()) evaluated on
   // the device state.
-  void field_out(const std::string& fname, unsigned step) { check(tsp_write_field(h_, 0, fname.c_str(), step), h_); }
+  void field_out(const std::string& fname, unsigned step) {
+    flush();
+    check(tsp_write_field(h_, 0, fname.c_str(), step), h_);
+  }
   double L2error(const std::function<std::array<double, 2>(double, double)>& uex) {
+    flush();
     const Mesh& m = *Xh_->mesh();
     const int32_t ne = int32_t(m.ne()), nq = (Xh_->degree() + 1) * (Xh_->degree() + 1);
     std::vector<double> pts(size_t(ne) * nq * 2), ex(size_t(ne) * nq * 2);
@@ -326,20 +349,25 @@ class LeapFrog {
     return err;
   }
   // TimeAdvance::eval_receivers (TimeAdvance.cpp:68-79): the device samples
-  // every step; this records which steps are written out.
+  // every step; this records which steps are written out (no device work).
   void eval_receivers() {
-    int64_t k = 0;
-    check(tsp_get_progress(h_, &k, nullptr), h_);
-    sampled_.push_back(k - 1);
+    if (!h_) throw Error(TSP_ERR_STATE, "eval_receivers before first_step");
+    sampled_.push_back(steps_ - 1);
   }
   // Receivers::write (Receivers.cpp:32-46): <fn>_rcv_<i>.out, "ux uy" lines.
+  // The samples of every recorded step come back in one read.
   void write_receivers(const std::string& fn) {
+    flush();
     const unsigned nr = rcv_.size();
     std::vector<std::vector<std::array<double, 2>>> rows(nr);
-    std::vector<double> buf(size_t(nr) * 2);
-    for (int64_t k : sampled_) {
-      check(tsp_get_seismograms(h_, k, 1, buf.data()), h_);
-      for (unsigned i = 0; i < nr; ++i) rows[i].push_back({buf[2 * i], buf[2 * i + 1]});
+    int64_t nk = 0;
+    for (int64_t k : sampled_) nk = std::max<int64_t>(nk, k + 1);
+    if (nr > 0 && nk > 0) {
+      if (nk > seis_cap_) throw Error(TSP_ERR_STATE, "receiver samples beyond the recorded run length");
+      std::vector<double> buf(size_t(nk) * nr * 2);
+      check(tsp_get_seismograms(h_, 0, nk, buf.data()), h_);
+      for (int64_t k : sampled_)
+        for (unsigned i = 0; i < nr; ++i) rows[i].push_back({buf[(size_t(k) * nr + i) * 2], buf[(size_t(k) * nr + i) * 2 + 1]});
     }
     for (unsigned i = 0; i < nr; ++i) {
       std::ofstream o(fn + "_rcv_" + std::to_string(i) + ".out");
@@ -348,7 +376,11 @@ class LeapFrog {
       for (auto& v : rows[i]) o << v[0] << " " << v[1] << "\n";
     }
   }
-  tsp_handle* handle() const { return h_; }
+  // The engine handle, with every queued step run.
+  tsp_handle* handle() {
+    flush();
+    return h_;
+  }
 
  private:
   void build() {
@@ -394,6 +426,7 @@ class LeapFrog {
     }
     check(tsp_set_force_table(h_, 0, F.data(), n), h_);
     check(tsp_set_seismogram_capacity(h_, n), h_);
+    seis_cap_ = n;
   }
 
   FESpace_ptr Xh_;
@@ -402,6 +435,7 @@ class LeapFrog {
   int precision_, device_;
   tsp_handle* h_ = nullptr;
   double dt_ = 0, tmax_ = 0, penalty_ = 2.0, last_time_ = 0;
+  int64_t steps_ = 0, pending_ = 0, seis_cap_ = 0;
   bool completed_ = false, dirty_ = true;
   Force_ptr force_;
   std::vector<double> u0_, v0_, uh_;

@@ -15,10 +15,11 @@ def test_reference_arm_prints_the_contract_line():
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "tsp_ref_run")):
         pytest.skip("reference build absent (oracle/Makefile)")
     res = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                          "--warmup", "0", "--ref-scale", "0.2"], capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert res.returncode == 0, res.stderr[-2000:]
     line = json.loads(res.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
+    assert "x0.2" in line["sample"] and line["sample"] == line["cpu_baseline"]["sample"]
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "config",
                 "cpu_baseline", "e2e"):
         assert key in line, key

@@ -149,6 +149,100 @@ def test_autotuner_choice_and_override(monkeypatch):
         assert s.kernel_variant == 2
 
 
+def test_fp64_autotuner_choice_and_override(monkeypatch):
+    """FP64 with several shots: the autotuner times the FP64 kernels (5, 6
+    warp-specialised DMMA; 3 single-role DMMA; 2 CUDA cores) and keeps one;
+    TSP_BATCHED_VARIANT forces one; every choice gives the same results to
+    rounding."""
+    m = W.jittered_rect(8, 5, 800.0, 500.0, seed=33)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    shots = [(100.0 + 9 * k, 120.0 + 3 * (k % 50)) for k in range(40)]
+    rcv = W.surface_receivers(m, 4)
+    n = 40
+    out = {}
+    for forced in (None, "5", "6", "3", "2"):
+        if forced is None:
+            monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
+        else:
+            monkeypatch.setenv("TSP_BATCHED_VARIANT", forced)
+        with capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, shots, rcv, penalty=10.0) as s:
+            v = s.kernel_variant
+            assert v in (5, 6, 3, 2) if forced is None else v == int(forced)
+            s.set_dt(2e-4)
+            for k in range(len(shots)):
+                s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
+            s.first_step()
+            s.run(n - 1)
+            out[forced] = s.seismograms(0, n)
+    for forced in ("5", "6", "3"):
+        assert np.linalg.norm(out[forced] - out["2"]) <= 1e-13 * np.linalg.norm(out["2"])
+    assert np.linalg.norm(out[None] - out["2"]) <= 1e-13 * np.linalg.norm(out["2"])
+
+
+@pytest.mark.parametrize("precision,op,nshots,variant", [
+    ("fp64", "explicit", 1, None), ("fp64", "matrix_free", 1, None), ("fp64", "explicit", 3, "5"),
+    ("fp64", "explicit", 3, "6"), ("fp64", "explicit", 3, "3"), ("fp64", "explicit", 3, "2"),
+    ("fp32", "explicit", 1, None), ("fp32", "explicit", 3, "0"), ("fp32", "explicit", 3, "4")])
+def test_unstable_dt_is_reported_as_nonfinite(precision, op, nshots, variant, monkeypatch):
+    """A time step of 3x the CFL limit is an ordinary numerical blow-up: the
+    state overflows to Inf/NaN within a few hundred steps. Every step kernel
+    raises the device's non-finite flag, tsp_run_timed returns
+    TSP_ERR_NONFINITE (-7) and the watchdog reports it; new initial values
+    clear it and a stable run is clean again."""
+    if variant is None:
+        monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
+    else:
+        monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+    m = W.jittered_rect(5, 4, 500.0, 400.0, seed=12)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    shots = [(120.0 + 100 * k, 150.0 + 50 * k) for k in range(nshots)]
+    rng = np.random.default_rng(6)
+    with capi.Simulation.create(m.xy, m.tri, 3, lam, mu, rho, shots, W.surface_receivers(m, 2), penalty=10.0,
+                                precision=precision, op=op) as s:
+        dt_cfl = 2 / np.sqrt(s.estimate_lmax(200))
+        u0 = [1e-3 * rng.standard_normal(2 * s.ne * s.Np) for _ in range(nshots)]
+        s.set_dt(3 * dt_cfl)
+        for k in range(nshots):
+            s.set_initial(k, u0[k], None)
+        s.first_step()
+        with pytest.raises(capi.TspError) as e:
+            s.run_timed(600)
+        assert e.value.code == -7
+        assert not s.check_finite()
+        s.set_dt(0.4 * dt_cfl)
+        for k in range(nshots):
+            s.set_initial(k, u0[k], None)
+        s.first_step()
+        s.run_timed(100)
+        assert s.check_finite()
+
+
+def test_run_pieces_match_single_steps():
+    """tsp_run replays pieces of at most 256 steps (and the powers of two of
+    the remainder), so runs of many different lengths share a bounded set of
+    graphs: they give exactly the state and receiver samples of single
+    steps."""
+    m = W.jittered_rect(4, 3, 400.0, 300.0, seed=4)
+    lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
+    mk = lambda: capi.Simulation.create(m.xy, m.tri, 2, lam, mu, rho, [(150.0, 140.0)],  # noqa: E731
+                                        W.surface_receivers(m, 2), penalty=10.0)
+    with mk() as a, mk() as b:
+        for s in (a, b):
+            s.set_dt(2e-4)
+            s.set_ricker(0, 20.0, 0.05, -1.0, 1, 2000)
+            s.set_seismogram_capacity(2000)
+            s.first_step()
+        total = 1
+        for n in (1, 2, 3, 7, 255, 256, 257, 300, 511, 13):
+            a.run(n)
+            total += n
+        for _ in range(total - 1):
+            b.step()
+        assert a.progress() == b.progress()
+        assert np.array_equal(a.u(), b.u())
+        assert np.array_equal(a.seismograms(0, total), b.seismograms(0, total))
+
+
 def test_u_all_matches_per_shot_reads():
     """tsp_get_u_all (device transpose, chunked read-back) returns exactly the
     per-shot tsp_get_u vectors."""

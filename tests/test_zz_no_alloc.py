@@ -25,12 +25,31 @@ def _noalloc(sim, iters):
     return out.value
 
 
-@pytest.mark.parametrize("N,precision", [(2, "fp64"), (4, "fp32")])
-def test_noalloc_lmax_matches_allocating_entry_point(N, precision):
+def _mesh():
     m = W.jittered_rect(4, 3, 400.0, 300.0, seed=5)
     lam, mu, rho = W.lame(np.full(m.ne, 3000.0), np.full(m.ne, 1732.0), np.full(m.ne, 2200.0))
-    with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, [(150.0, 140.0)], [], penalty=10.0,
-                                precision=precision) as s:
+    return m, lam, mu, rho
+
+
+# One shot (explicit FP64 / FP32 blocks, the matrix-free operator) and several
+# shots (FP64 blocks at the batched pitch; FP32 blocks with the batched
+# kernels' state shadow): the estimate works on the operator alone, whatever
+# the handle's step kernels.
+CASES = [
+    (2, "fp64", "explicit", 1),
+    (4, "fp32", "explicit", 1),
+    (3, "fp64", "matrix_free", 1),
+    (4, "fp64", "explicit", 3),
+    (5, "fp32", "explicit", 3),
+]
+
+
+@pytest.mark.parametrize("N,precision,op,nshots", CASES)
+def test_noalloc_lmax_matches_allocating_entry_point(N, precision, op, nshots):
+    m, lam, mu, rho = _mesh()
+    shots = [(150.0, 140.0), (250.0, 100.0), (90.0, 200.0)][:nshots]
+    with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, [], penalty=10.0,
+                                precision=precision, op=op) as s:
         ref = s.estimate_lmax(2000)
         first = _noalloc(s, 2000)
         second = _noalloc(s, 2000)

@@ -365,8 +365,9 @@ class Simulation:
     def kernel_variant(self) -> int:
         """Batched-step kernel chosen by the autotuner (or TSP_BATCHED_VARIANT):
         FP32: 0/1/2 CUDA-core kernels, 4 tensor-core fixed-point kernel; FP64
-        with several shots: 5 warp-specialised FP64 tensor-core kernel, 3
-        single-role one, 2 CUDA-core kernel."""
+        with several shots: 5 and 6 warp-specialised FP64 tensor-core kernels
+        (two groups of 8 consumer warps / one group of 16), 3 single-role
+        one, 2 CUDA-core kernel."""
         v = C.c_int32()
         _check(lib().tsp_get_kernel_variant(self._h, C.byref(v)), self._h)
         return v.value

@@ -1,6 +1,7 @@
 // C-ABI of the tspeed_b200 engine (include/tspeed_b200.h).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -21,6 +22,7 @@
 #include "tsp_tcgen05.cuh"
 #include "tsp_tcfx.cuh"
 #include "tsp_dmma.cuh"
+#include "tsp_simt32.cuh"
 
 namespace {
 
@@ -81,7 +83,10 @@ struct tsp_handle {
   int* d_Bex = nullptr;
   unsigned char* d_Xsl[2] = {nullptr, nullptr};
   int* d_Xex[2] = {nullptr, nullptr};
-  int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
+  // [0] set by a kernel whose bounded wait gave up; [1] set by a step kernel
+  // that wrote a NaN or infinite displacement (cleared by new initial values
+  // or a resumed state).
+  int* d_err = nullptr;
   int num_sms = 148;
   long long* d_step = nullptr;
   // sources / receivers
@@ -106,11 +111,21 @@ struct tsp_handle {
   long long steps_done = 0;
   double last_time = 0.0;
   std::string err = "no error";
-  std::map<std::pair<long long, int>, cudaGraphExec_t> graphs;
+  std::map<std::pair<long long, int>, cudaGraphExec_t> graphs;  // (steps, parity) -> tsp_run piece
   std::vector<void*> owned;  // device allocations, freed at destroy
 };
 
 namespace {
+
+// NVTX range over a scope: set-up, uploads, the step loop and read-backs show
+// up by name in a profiler's timeline (header-only NVTX; a no-op without a
+// tool attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 int fail(tsp_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -233,6 +248,9 @@ void to_ref_coords(const tsp_handle* h, double* v, long long nvec) {
   if (!h->lref_inv.empty()) map_vectors(h->lref_inv, true, h->Np, v, nvec);
 }
 
+// Longest graph tsp_run captures (steps); longer runs replay it.
+constexpr long long kRunChunk = 256;
+
 void clear_graphs(tsp_handle* h) {
   for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
   h->graphs.clear();
@@ -316,23 +334,36 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
                 double xscale, cudaStream_t st);
 int check_device_error(tsp_handle* h);
 
-// Autotuner of the batched FP32 step: each applicable kernel variant (tile
-// shape, shots per CTA, CUDA cores or tensor cores) runs a few steps on the
-// zero initial state of the handle -- no sources are set yet, so every
-// output stays zero and nothing needs restoring -- timed with CUDA events on
-// the handle's stream; the fastest is kept. TSP_BATCHED_VARIANT skips it.
-// Choices are kept per process for handles of the same shape (device,
-// 2Np, shots, elements): a second handle of the same problem skips the trials.
+// Autotuner of the batched step kernels: each applicable kernel variant
+// (tile shape, shots per CTA, ring depth, CUDA cores or tensor cores) runs a
+// few steps on the zero initial state of the handle -- no sources are set
+// yet, so every output stays zero and nothing needs restoring -- timed with
+// CUDA events on the handle's stream; the fastest is kept. FP32 operator
+// (with its FP32 state shadow): 7 warp-specialised with bulk-copy rings and
+// 8 shots x several rows per lane, 0 K split over warp groups, 1 pipelined
+// single group, 2 non-persistent, 4 tensor-core fixed point. FP64 operator: 5 and 6
+// warp-specialised DMMA (two consumer groups of 8 warps, or one group of 16
+// warps with a latency-free epilogue), 3 single-role DMMA, 2 CUDA cores. TSP_BATCHED_VARIANT skips
+// the trials. Choices are kept per process for handles of the same shape
+// (device, precision, 2Np, shots, elements): a second handle of the same
+// problem skips the trials.
 std::mutex g_tune_mutex;
-std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+std::map<std::tuple<int, int, int, int, int>, int> g_tune_cache;
 
 int autotune(tsp_handle* h) {
+  NvtxRange nvtx_("autotune");
   const bool fx_ok = h->fx;
-  if (h->kernel_variant >= 0 || !h->shadow) {
+  const bool fp64_batched = h->S > 1 && h->prec == TSP_PREC_FP64 && h->op_kind == TSP_OP_EXPLICIT;
+  if (fp64_batched) {
+    if (h->kernel_variant >= 0) {
+      if (h->kernel_variant != 2 && h->kernel_variant != 3 && h->kernel_variant != 6) h->kernel_variant = 5;
+      return TSP_OK;
+    }
+  } else if (h->kernel_variant >= 0 || !h->shadow) {
     if (h->kernel_variant < 0) h->kernel_variant = 0;
     return TSP_OK;
   }
-  const auto key = std::make_tuple(h->device, h->R, h->S, h->ne);
+  const auto key = std::make_tuple(h->device, h->prec, h->R, h->S, h->ne);
   int cached = -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mutex);
@@ -340,8 +371,9 @@ int autotune(tsp_handle* h) {
     if (it != g_tune_cache.end()) cached = it->second;
   }
   std::vector<int> cands;
-  if (h->R <= 42) cands = {0, 1, 2};
-  else if (h->R <= 56) cands = {0, 2};
+  if (fp64_batched) cands = {5, 6, 3, 2};
+  else if (h->R <= 42) cands = {7, 0, 1, 2};
+  else if (h->R <= 56) cands = {7, 0, 2};
   else cands = {2};
   if (fx_ok) cands.push_back(4);
   if (cached >= 0 && (cached != 4 || fx_ok)) cands = {cached};
@@ -441,8 +473,8 @@ int finish_create(tsp_handle* h) {
   if (h->fx && (rc = fx_dispatch(h, true, 0))) return rc;
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
-  if ((rc = dalloc(h, &h->d_err, 1))) return rc;
-  TSP_CUDA(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+  if ((rc = dalloc(h, &h->d_err, 2))) return rc;
+  TSP_CUDA(h, cudaMemsetAsync(h->d_err, 0, 2 * sizeof(int), h->stream));
   if ((rc = dalloc(h, &h->d_acc, 3))) return rc;
   if ((rc = upload(h, &h->d_src_elem, h->src_elem.data(), h->src_elem.size()))) return rc;
   {
@@ -497,31 +529,37 @@ int launch_d64(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   return TSP_OK;
 }
 
-template <int R>
+// FP64 warp-specialised DMMA step, two configurations (autotuner
+// candidates): V = 5, two consumer groups of 8 warps alternating items (one
+// group's epilogue, with its global loads, overlaps the other's products),
+// each warp one m-tile of 8 shots x every operator row, a ring of its own per
+// group (2Np <= 56; one group for 2Np = 72 and 90, whose stages fit fewer
+// times); V = 6, one group of 16 warps, each 8 shots x half the rows, whose
+// epilogue reads u^k from shared memory and u^{k-1} from loads requested
+// before the products, so it has no latency to hide.
+template <int R, int V>
 int launch_d64w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
-  // Each consumer warp owns one m-tile of 8 shots and every operator row
-  // (all n-tiles) when the tile has 64 shots: measured fastest at 2Np = 42
-  // (1.55 ms per step against 1.71 for 2 m-tiles x half the rows). For
-  // 2Np > 56 a stage no longer fits five times in shared memory: one consumer
-  // group with a 3-stage (2Np = 72) or 2-stage (2Np = 90) ring.
-  constexpr int NG = R <= 56 ? 2 : 1;
-  constexpr int NST = R <= 56 ? 5 : (R <= 72 ? 3 : 2);
-  constexpr int WM = tsp::D64WCfg<R, NST, NG>::ST / 8, WN = 8 / WM;
-  typedef tsp::D64WCfg<R, NST, NG, WM, WN> CF;
+  constexpr int NG = (V == 5 && R <= 56) ? 2 : 1;
+  constexpr int ST = tsp::D64WCfg<R, 1, NG>::ST;
+  constexpr int NCW = (V == 5) ? 8 : 16;
+  constexpr int WM = ST / 8, WN = NCW / WM;
+  constexpr int EPI = (V == 5) ? 0 : 1;
+  constexpr int NSG = tsp::d64w_fit_nsg<R, NG, WM, WN, (NG == 1 ? 6 : 4)>();
+  static_assert(NSG >= 2, "FP64 DMMA ring: two stages per group must fit");
+  typedef tsp::D64WCfg<R, NSG, NG, WM, WN> CF;
   const size_t smem = CF::smem_bytes();
   static unsigned long long configured = 0;  // one bit per device
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e =
-        cudaFuncSetAttribute(tsp::k_step_batched64w<R, NST, NG, 1, WM, WN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem));
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP64 batched kernel smem: ") + cudaGetErrorString(e));
     configured |= bit;
   }
   // Persistent: one CTA per SM.
   const long long items = (long long)h->ne * ((h->S + CF::ST - 1) / CF::ST);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
-  tsp::k_step_batched64w<R, NST, NG, 1, WM, WN><<<grid, CF::NT, smem, st>>>(p, h->d_err);
+  tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI><<<grid, CF::NT, smem, st>>>(p, h->d_err);
   return TSP_OK;
 }
 
@@ -597,6 +635,33 @@ int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   return TSP_OK;
 }
 
+// FP32-operator step on the CUDA cores with warp-specialised bulk-copy rings
+// (variant 7): 6 consumer warps in groups of NWG (one or two warps per item),
+// a ring per group. Seven warps per CTA leave each thread up to 255
+// registers: the 8-shot x RL-row tiles and the FP64 epilogue fit without
+// spills (nine warps cap a thread at 168 registers and spill).
+template <int R>
+int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  constexpr int NWG = tsp::S32WCfg<R>::NWG;
+  constexpr int NGR = 6 / NWG;
+  constexpr int NSG = tsp::s32w_fit_nsg<R, NGR>();
+  static_assert(NSG >= 2, "FP32 ring: two stages per group must fit");
+  typedef tsp::S32WLayout<R, NGR, NSG> LY;
+  const size_t smem = LY::smem_bytes();
+  static unsigned long long configured = 0;
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP32 ring kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  const long long items = (long long)h->ne * ((h->S + 63) / 64);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched32w<R, NGR, NSG><<<grid, LY::NT, smem, st>>>(p, h->d_err);
+  return TSP_OK;
+}
+
 template <int R>
 int launch_ksplit(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::KsplitCfg<R> CF;
@@ -619,6 +684,9 @@ template <int R>
 int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   if constexpr (R <= 56) {
     if (h->fx && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) return launch_fx<R>(h, p, st);
+  }
+  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant == 7) {
+    if constexpr (R <= 56) return launch_s32w<R>(h, p, st);
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 42) {
@@ -643,12 +711,15 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
     tsp::k_step_batched32<R><<<grid, CF::NT, smem, st>>>(p);
     return TSP_OK;
   }
-  // FP64 with several shots: the FP64 tensor-core (DMMA) kernels, the
-  // warp-specialised persistent one by default; TSP_BATCHED_VARIANT=3 selects
-  // the single-role DMMA kernel and 2 the register-staged CUDA-core kernel.
+  // FP64 with several shots: the FP64 tensor-core (DMMA) kernels, chosen by
+  // the autotuner or TSP_BATCHED_VARIANT: 5 and 6 the warp-specialised
+  // persistent kernel (two warp tiles), 3 the single-role DMMA kernel, 2 the
+  // register-staged CUDA-core kernel.
   if (h->S > 1 && h->prec == TSP_PREC_FP64 && h->kernel_variant != 2 &&
       (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
-    return h->kernel_variant == 3 ? launch_d64<R>(h, p, st) : launch_d64w<R>(h, p, st);
+    return h->kernel_variant == 3 ? launch_d64<R>(h, p, st)
+           : h->kernel_variant == 6 ? launch_d64w<R, 6>(h, p, st)
+                                    : launch_d64w<R, 5>(h, p, st);
   if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::BatchCfg<R> CF;
     const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));
@@ -711,6 +782,7 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
   p.nrcv = h->nrcv;
   p.seis_cap = h->seis_cap;
   p.energy = (sample && h->energy_on) ? h->d_energy : nullptr;
+  p.nonfinite = sample ? h->d_err + 1 : nullptr;
   p.energy_cap = h->energy_cap;
   p.acc = h->d_acc;
   p.x32_in = nullptr;
@@ -810,6 +882,26 @@ int check_device_error(tsp_handle* h) {
   return TSP_OK;
 }
 
+// Reads the non-finite flag of the step kernels (synchronises the stream).
+int read_nonfinite(tsp_handle* h, int* v) {
+  *v = 0;
+  if (!h->d_err) return TSP_OK;
+  TSP_CUDA(h, copy_sync(v, h->d_err + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  return TSP_OK;
+}
+int check_nonfinite(tsp_handle* h) {
+  int v = 0, rc = read_nonfinite(h, &v);
+  if (rc) return rc;
+  if (v)
+    return fail(h, TSP_ERR_NONFINITE,
+                "a step produced a NaN or infinite displacement (dt above the stability limit, or bad inputs)");
+  return TSP_OK;
+}
+int reset_nonfinite(tsp_handle* h) {
+  if (h->d_err) TSP_CUDA(h, cudaMemsetAsync(h->d_err + 1, 0, sizeof(int), h->stream));
+  return TSP_OK;
+}
+
 // One shot's slice of a device state buffer (ne runs of R doubles with a
 // stride of S*R) to/from a reference-layout host vector (NULL: zeros).
 int get_shot(tsp_handle* h, const double* dsrc, int shot, double* out) {
@@ -883,6 +975,7 @@ const char* tsp_version(void) { return "tspeed_b200 0.1 sm_100a"; }
 const char* tsp_last_error(const tsp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
 int tsp_create(const tsp_problem* P, tsp_handle** out) {
+  NvtxRange nvtx_("tsp_create");
   if (!P || !out) return fail(nullptr, TSP_ERR_ARG, "null argument");
   *out = nullptr;
   if (P->N < 1 || P->N > tsp::kMaxN) return fail(nullptr, TSP_ERR_UNSUPPORTED, "degree N must be in 1..8");
@@ -1102,6 +1195,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
 }
 
 int tsp_create_from_blocks(const tsp_block_problem* P, tsp_handle** out) {
+  NvtxRange nvtx_("tsp_create_from_blocks");
   if (!P || !out) return fail(nullptr, TSP_ERR_ARG, "null argument");
   *out = nullptr;
   if (P->ne <= 0 || P->Np <= 0 || P->nnzb < P->ne || !P->row_ptr || !P->col || !P->blocks || !P->minv)
@@ -1268,6 +1362,7 @@ int tsp_force_times(double dt, int64_t n, double* out) {
 }
 
 int tsp_set_force_table(tsp_handle* h, int32_t shot, const double* F, int64_t n) {
+  NvtxRange nvtx_("tsp_set_force_table");
   if (!h) return TSP_ERR_ARG;
   if (shot < 0 || shot >= h->S || n < 0 || (n > 0 && !F)) return fail(h, TSP_ERR_ARG, "bad force table");
   int rc;
@@ -1307,6 +1402,7 @@ int tsp_set_ricker(tsp_handle* h, int32_t shot, double f0, double t0, double amp
 }
 
 int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double* v0) {
+  NvtxRange nvtx_("tsp_set_initial");
   if (!h) return TSP_ERR_ARG;
   if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
   int rc;
@@ -1326,12 +1422,14 @@ int tsp_set_initial(tsp_handle* h, int32_t shot, const double* u0, const double*
   h->steps_done = 0;
   h->last_time = 0.0;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  if ((rc = reset_nonfinite(h))) return rc;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
   clear_graphs(h);
   return TSP_OK;
 }
 
 int tsp_first_step(tsp_handle* h) {
+  NvtxRange nvtx_("tsp_first_step");
   if (!h) return TSP_ERR_ARG;
   if (!h->dt_set) return fail(h, TSP_ERR_STATE, "first_step needs dt (tsp_set_dt)");
   int rc;
@@ -1353,6 +1451,7 @@ int tsp_first_step(tsp_handle* h) {
 }
 
 int tsp_step(tsp_handle* h) {
+  NvtxRange nvtx_("tsp_step");
   if (!h) return TSP_ERR_ARG;
   if (h->steps_done < 1) return fail(h, TSP_ERR_STATE, "step before first_step");
   int rc;
@@ -1369,41 +1468,60 @@ int tsp_step(tsp_handle* h) {
 }
 
 int tsp_run(tsp_handle* h, int64_t nsteps) {
+  NvtxRange nvtx_("tsp_run");
   if (!h) return TSP_ERR_ARG;
   if (nsteps < 0) return fail(h, TSP_ERR_ARG, "negative step count");
   if (nsteps == 0) return TSP_OK;
   if (h->steps_done < 1) return fail(h, TSP_ERR_STATE, "run before first_step");
   int rc;
   if ((rc = begin(h))) return rc;
-  const auto key = std::make_pair((long long)nsteps, h->cur);
-  auto it = h->graphs.find(key);
-  if (it == h->graphs.end()) {
-    cudaGraph_t graph;
-    TSP_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int c = h->cur;
-    int lrc = TSP_OK;
-    for (int64_t i = 0; i < nsteps && lrc == TSP_OK; ++i) {
-      lrc = launch_step(h, tsp::kModeStep, h->d_U[c], h->d_U[1 - c], h->d_U[1 - c], int(i), 1.0, h->stream);
-      c = 1 - c;
+  // The run is a sequence of pieces, each a replay of a cached graph of
+  // kRunChunk steps or of a power of two below it (the binary digits of the
+  // remainder): at most 2 x (1 + log2 kRunChunk) graphs per handle, keyed by
+  // length and the parity of the current level, whatever step counts the
+  // caller asks for. Steps of a piece read the device step counter plus their
+  // offset, and the piece advances the counter, so pieces replay anywhere in
+  // time.
+  int c = h->cur;
+  for (int64_t left = nsteps; left > 0;) {
+    long long len = kRunChunk;
+    if (left < kRunChunk) {
+      len = 1;
+      while (len * 2 <= left) len *= 2;
     }
-    tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, nsteps);
-    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
-    if (lrc) return lrc;
-    if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-    cudaGraphExec_t exec;
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-    it = h->graphs.emplace(key, exec).first;
+    const auto key = std::make_pair(len, c);
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+      cudaGraph_t graph;
+      TSP_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      int cc = c;
+      int lrc = TSP_OK;
+      for (long long i = 0; i < len && lrc == TSP_OK; ++i) {
+        lrc = launch_step(h, tsp::kModeStep, h->d_U[cc], h->d_U[1 - cc], h->d_U[1 - cc], int(i), 1.0, h->stream);
+        cc = 1 - cc;
+      }
+      tsp::k_advance<<<1, 1, 0, h->stream>>>(h->d_step, len);
+      cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+      if (lrc) return lrc;
+      if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      cudaGraphExec_t exec;
+      ce = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      it = h->graphs.emplace(key, exec).first;
+    }
+    TSP_CUDA(h, cudaGraphLaunch(it->second, h->stream));
+    if (len & 1) c = 1 - c;
+    left -= len;
   }
-  TSP_CUDA(h, cudaGraphLaunch(it->second, h->stream));
-  if (nsteps & 1) h->cur = 1 - h->cur;
+  h->cur = c;
   h->steps_done += nsteps;
   for (int64_t i = 0; i < nsteps; ++i) h->last_time = h->last_time + h->dt;
   return TSP_OK;
 }
 
 int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
+  NvtxRange nvtx_("tsp_run_timed");
   if (!h || !ms) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
@@ -1420,6 +1538,7 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
     if (e != cudaSuccess) rc = fail(h, TSP_ERR_CUDA, std::string("timing events: ") + cudaGetErrorString(e));
     *ms = f;
     if (rc == TSP_OK) rc = check_device_error(h);
+    if (rc == TSP_OK) rc = check_nonfinite(h);
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -1428,12 +1547,9 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms) {
 
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant) {
   if (!h || !variant) return TSP_ERR_ARG;
+  // FP64 with several shots: 2 CUDA-core, 3 single-role DMMA, 5 and 6 the
+  // warp-specialised DMMA kernel (two warp tiles); set by the autotuner.
   *variant = h->kernel_variant;
-  // FP64 with several shots: 2 CUDA-core, 3 single-role DMMA, else the
-  // warp-specialised DMMA kernel, reported as 5.
-  if (h->prec == TSP_PREC_FP64 && h->S > 1 && h->op_kind == TSP_OP_EXPLICIT && h->kernel_variant != 2 &&
-      h->kernel_variant != 3)
-    *variant = 5;
   return TSP_OK;
 }
 
@@ -1445,6 +1561,7 @@ int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time
 }
 
 int tsp_get_u(tsp_handle* h, int32_t shot, double* out) {
+  NvtxRange nvtx_("tsp_get_u");
   if (!h || !out) return TSP_ERR_ARG;
   if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
   int rc;
@@ -1454,6 +1571,7 @@ int tsp_get_u(tsp_handle* h, int32_t shot, double* out) {
 }
 
 int tsp_get_u_all(tsp_handle* h, double* out) {
+  NvtxRange nvtx_("tsp_get_u_all");
   if (!h || !out) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
@@ -1490,6 +1608,7 @@ int tsp_set_seismogram_capacity(tsp_handle* h, int64_t nsteps) {
 }
 
 int tsp_get_seismograms(tsp_handle* h, int64_t k0, int64_t nk, double* out) {
+  NvtxRange nvtx_("tsp_get_seismograms");
   if (!h) return TSP_ERR_ARG;
   if (k0 < 0 || nk < 0 || (nk > 0 && !out)) return fail(h, TSP_ERR_ARG, "bad range");
   if (nk > h->seis_cap) return fail(h, TSP_ERR_ARG, "range longer than the seismogram capacity");
@@ -1542,6 +1661,7 @@ int tsp_get_energy(tsp_handle* h, int64_t k0, int64_t nk, double* out) {
 }
 
 int tsp_get_state(tsp_handle* h, double* u_prev, double* u_cur, int64_t* steps_done, double* last_time) {
+  NvtxRange nvtx_("tsp_get_state");
   if (!h) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
@@ -1561,6 +1681,7 @@ int tsp_get_state(tsp_handle* h, double* u_prev, double* u_cur, int64_t* steps_d
 }
 
 int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int64_t steps_done, double last_time) {
+  NvtxRange nvtx_("tsp_set_state");
   if (!h || !u_prev || !u_cur) return TSP_ERR_ARG;
   if (steps_done < 1) return fail(h, TSP_ERR_ARG, "a resumable state has at least one step done");
   int rc;
@@ -1578,6 +1699,7 @@ int tsp_set_state(tsp_handle* h, const double* u_prev, const double* u_cur, int6
   if ((rc = refresh_shadow(h, 1))) return rc;
   h->steps_done = steps_done;
   h->last_time = last_time;
+  if ((rc = reset_nonfinite(h))) return rc;
   long long sd = steps_done;
   TSP_CUDA(h, copy_sync(h->d_step, &sd, sizeof(sd), cudaMemcpyHostToDevice, h->stream));
   clear_graphs(h);
@@ -1592,12 +1714,13 @@ int tsp_check_finite(tsp_handle* h, int32_t* bad) {
   std::vector<double> all(nstate);
   TSP_CUDA(h, cudaMemcpyAsync(all.data(), h->d_U[h->cur], nstate * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
-  *bad = 0;
-  for (double v : all)
-    if (!std::isfinite(v)) {
-      *bad = 1;
-      break;
-    }
+  // The step kernels' flag (any non-finite value written since the initial
+  // values were set), or a non-finite value in the current level.
+  int flag = 0;
+  if ((rc = read_nonfinite(h, &flag))) return rc;
+  *bad = flag ? 1 : 0;
+  for (size_t i = 0; i < all.size() && !*bad; ++i)
+    if (!std::isfinite(all[i])) *bad = 1;
   return TSP_OK;
 }
 
@@ -1631,6 +1754,7 @@ int tsp_apply(tsp_handle* h, const double* x, double* y) {
 }
 
 int tsp_estimate_lmax(tsp_handle* h, int32_t iters, double* lmax) {
+  NvtxRange nvtx_("tsp_estimate_lmax");
   if (!h || !lmax || iters < 1) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
@@ -1863,6 +1987,7 @@ int tsp_l2_error(tsp_handle* h, int32_t shot, const double* exact, double* err) 
 }
 
 int tsp_set_initial_values(tsp_handle* h, int32_t shot, const double* u_vals, const double* v_vals) {
+  NvtxRange nvtx_("tsp_set_initial_values");
   if (!h) return TSP_ERR_ARG;
   if (shot < 0 || shot >= h->S) return fail(h, TSP_ERR_ARG, "shot out of range");
   if (h->detJ.empty()) return fail(h, TSP_ERR_UNSUPPORTED, "the projection needs the mesh (handle built from blocks)");
@@ -1911,6 +2036,7 @@ int tsp_set_initial_values(tsp_handle* h, int32_t shot, const double* u_vals, co
   h->steps_done = 0;
   h->last_time = 0.0;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+  if ((rc = reset_nonfinite(h))) return rc;
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
   clear_graphs(h);
   return TSP_OK;
@@ -2077,11 +2203,6 @@ namespace {
 constexpr size_t kNoAllocScratchDoubles = size_t(4) << 20;  // 4 Mi doubles = 32 MiB
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
-// Device addresses of g_noalloc_scratch, one per device (host code may not use
-// the symbol itself as a device pointer).
-constexpr int kNoAllocMaxDevices = 64;
-double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
-
 __global__ void k_noalloc_start_vector(double* x, size_t n) {
   // Deterministic start vector with all modes excited (splitmix64 of the index).
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
@@ -2099,23 +2220,25 @@ extern "C" int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* l
   if (!h || !lmax || iters < 1) return TSP_ERR_ARG;
   int rc;
   if ((rc = begin(h))) return rc;
-  if (h->device < 0 || h->device >= kNoAllocMaxDevices)
-    return fail(h, TSP_ERR_UNSUPPORTED, "tsp_estimate_lmax_noalloc supports device ordinals 0..63");
+  if (h->nmesh > 0)
+    return fail(h, TSP_ERR_UNSUPPORTED,
+                "tsp_estimate_lmax_noalloc: multi-mesh groups estimate per mesh (tsp_batch_estimate_lmax)");
   const size_t n1 = size_t(h->ne) * h->R;  // one vector, layout [e][R]
   if (2 * n1 + 3 > kNoAllocScratchDoubles)
     return fail(h, TSP_ERR_ARG,
                 "tsp_estimate_lmax_noalloc: 2*ne*2Np + 3 = " + std::to_string(2 * n1 + 3) +
                     " doubles exceed the fixed scratch of " + std::to_string(kNoAllocScratchDoubles) +
                     " doubles (32 MiB); use tsp_estimate_lmax");
-  // One-time set-up per device, with that device current (begin() set it).
-  if (!g_noalloc_ptr[h->device]) {
-    void* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return fail(h, TSP_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-    g_noalloc_ptr[h->device] = static_cast<double*>(ptr);
-  }
-  double* da = g_noalloc_ptr[h->device];
+  // Device address of the array in the current context (begin() made the
+  // handle's device current). Looked up on every call -- a cheap host query
+  // -- so that no address outlives a context reset and concurrent callers
+  // share no host state. Host code cannot use the symbol itself as a device
+  // pointer.
+  void* ptr = nullptr;
+  cudaError_t ge = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (ge != cudaSuccess)
+    return fail(h, TSP_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(ge));
+  double* da = static_cast<double*>(ptr);
   double* db = da + n1;
   double* dacc = db + n1;
   k_noalloc_start_vector<<<592, 256, 0, h->stream>>>(da, n1);
@@ -2203,6 +2326,7 @@ int tsp_batch_destroy(tsp_batch* b) {
 const char* tsp_batch_last_error(const tsp_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
 
 int tsp_batch_create(const tsp_problem* meshes, int32_t nmesh, tsp_batch** out) {
+  NvtxRange nvtx_("tsp_batch_create");
   if (!meshes || !out || nmesh < 1) return bfail(nullptr, TSP_ERR_ARG, "need nmesh >= 1 problems");
   *out = nullptr;
   const int prec = meshes[0].precision, op = meshes[0].op_kind, dev = meshes[0].device;
@@ -2481,6 +2605,7 @@ int tsp_batch_first_step(tsp_batch* b) {
 
 // All groups' steps in one graph, replayed on the batch stream.
 int tsp_batch_run(tsp_batch* b, int64_t nsteps) {
+  NvtxRange nvtx_("tsp_batch_run");
   if (!b || nsteps < 0) return TSP_ERR_ARG;
   if (nsteps == 0) return TSP_OK;
   cudaSetDevice(b->device);

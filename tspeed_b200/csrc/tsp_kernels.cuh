@@ -81,7 +81,16 @@ struct StepParams {
   int* xex_out;
   const void* bsl;
   const int* bex;
+  // Non-finite watchdog (step modes only; null otherwise): set to 1 by any
+  // kernel that writes a NaN or infinite u^{k+1}.
+  int* nonfinite;
 };
+
+// Raises the non-finite flag when a new displacement pair holds a NaN or an
+// infinity (the leap-frog recurrence keeps such a value for good).
+__device__ __forceinline__ void note_nonfinite(const StepParams& p, double a, double b) {
+  if (!(isfinite(a) && isfinite(b)) && p.nonfinite != nullptr) *p.nonfinite = 1;
+}
 
 // ---------------------------------------------------------------------------
 // Loads. Operator blocks are streamed once per step: ld.global.cs keeps them
@@ -293,6 +302,7 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
         }
       }
       *reinterpret_cast<double2*>(o) = make_double2(unew[s][0], unew[s][1]);
+      note_nonfinite(p, unew[s][0], unew[s][1]);
       if (p.energy != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -523,6 +533,7 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
           }
         }
         *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+        note_nonfinite(p, un[0], un[1]);
       }
     }
   }
@@ -755,6 +766,7 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
         }
       }
       *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+      note_nonfinite(p, un[0], un[1]);
     }
   }
 
@@ -917,6 +929,7 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
           sh32[2 * jp + h][i] = float(un[h]);
         }
         *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
+        note_nonfinite(p, un[0], un[1]);
       }
     }
     float* gx = p.x32_out + (size_t(e) * ntile + tile) * R * ST + 4 * tx;
@@ -1154,6 +1167,7 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
         Hs[r * HP + sl] = float(un[h]);
       }
       *reinterpret_cast<double2*>(p.out + (size_t(e) * S + sh) * R + r0) = make_double2(un[0], un[1]);
+      note_nonfinite(p, un[0], un[1]);
     }
     __syncthreads();
     {
@@ -1341,6 +1355,7 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
         Hs[r * HP + sl] = float(un[h]);
       }
       *reinterpret_cast<double2*>(p.out + me) = make_double2(un[0], un[1]);
+      note_nonfinite(p, un[0], un[1]);
     }
     __syncthreads();
     {
@@ -1692,6 +1707,7 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
           pe2 += un * un;
         }
         og[r] = un;
+        note_nonfinite(p, un, 0.0);
       }
     }
     (void)ew;

@@ -128,8 +128,13 @@ __device__ __forceinline__ void fx_epi_sync() {
 
 // Shared exponent of a row whose largest magnitude is m: 2^(ex-1) <= m < 2^ex,
 // read from the bits (zero, subnormal, infinite and NaN rows: kNoExp, i.e.
-// the row counts as zero).
+// the row counts as zero). A state row holding a NaN or an infinity, or a
+// value of 2^1000 or more (a run that is overflowing), gets kNaNExp instead:
+// its slices are zero and its scale is NaN, so every product it enters
+// becomes NaN and the neighbours' rows carry the failure on, as the FP64
+// recurrence would.
 constexpr int kNoExp = -2147483647 - 1;
+constexpr int kNaNExp = 2147483647;
 __device__ __forceinline__ int fx_exponent(double m) {
   const int f = int((__double_as_longlong(m) >> 52) & 0x7FF);
   return (f == 0 || f == 0x7FF) ? kNoExp : f - 1022;
@@ -142,7 +147,9 @@ __device__ __forceinline__ double fx_factor24(int ex) { return fx_valid(ex) ? fx
 // Row scales of a block product whose class sum is counted in units of
 // 2^-8: 2^(ex-8) * 2^(eb-8) * 2^-8 = fx_shot_scale(ex) * fx_row_scale(eb)
 // (0 for a zero row).
-__device__ __forceinline__ double fx_shot_scale(int ex) { return fx_valid(ex) ? fx_pow2(ex - 24) : 0.0; }
+__device__ __forceinline__ double fx_shot_scale(int ex) {
+  return fx_valid(ex) ? fx_pow2(ex - 24) : (ex == kNaNExp ? __longlong_as_double(0x7FF8000000000000ll) : 0.0);
+}
 __device__ __forceinline__ double fx_row_scale(int eb) { return fx_valid(eb) ? fx_pow2(eb) : 0.0; }
 
 // BF16 bits of q * scale for a small integer q (|q| <= 256) and a power of
@@ -576,8 +583,13 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
             Ys[s2 * YS + r] = un[h];
           }
           *reinterpret_cast<double2*>(p.out + (size_t(e) * S + sh) * R + r0) = make_double2(un[0], un[1]);
-          const double mx = fmax(fabs(un[0]), fabs(un[1]));
-          if (mx > 0.0) atomicMax(&shexp[s2], fx_exponent(mx));
+          if (isfinite(un[0]) && isfinite(un[1])) {
+            const double mx = fmax(fabs(un[0]), fabs(un[1]));
+            if (mx > 0.0) atomicMax(&shexp[s2], fx_exponent(mx));
+          } else {
+            atomicMax(&shexp[s2], kNaNExp);
+            if (p.nonfinite != nullptr) *p.nonfinite = 1;
+          }
         }
       }
       fx_epi_sync<NUPT>();
@@ -589,9 +601,11 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
       // ---- per-shot factors and scales of u^{k+1} on this element ----
       const size_t tix = size_t(e) * ntile + tile;
       if (ut < M && !dead) {
-        const int ex = (ut < nsv) ? shexp[ut] : kNoExp;
+        const int ex0 = (ut < nsv) ? shexp[ut] : kNoExp;
+        const int ex = ex0 > 1000 ? kNaNExp : ex0;
+        if (ex0 > 1000 && ex0 != kNaNExp && p.nonfinite != nullptr) *p.nonfinite = 1;
         shfac[ut] = fx_factor24(ex);
-        p.xex_out[tix * M + ut] = fx_valid(ex) ? ex : kNoExp;
+        p.xex_out[tix * M + ut] = (fx_valid(ex) || ex == kNaNExp) ? ex : kNoExp;
       }
       fx_epi_sync<NUPT>();
       // ---- slices of u^{k+1}: image of the shared-memory operand layout ----
@@ -711,10 +725,14 @@ __global__ void k_make_xslices(const double* __restrict__ u, int ne, int S, unsi
     }
     const double* ue = u + (size_t(e) * S + sh) * R;
     double m = 0.0;
-    for (int r = 0; r < R; ++r) m = fmax(m, fabs(ue[r]));
-    const int ex = fx_exponent(m);
+    bool fin = true;
+    for (int r = 0; r < R; ++r) {
+      m = fmax(m, fabs(ue[r]));
+      fin = fin && isfinite(ue[r]);
+    }
+    const int ex = (fin && fx_exponent(m) <= 1000) ? fx_exponent(m) : kNaNExp;
     const double fac = fx_factor24(ex);
-    xex[i] = fx_valid(ex) ? ex : kNoExp;
+    xex[i] = (fx_valid(ex) || ex == kNaNExp) ? ex : kNoExp;
     unsigned char* dst = img + size_t(tix) * CF::ABYTES;
     for (int r = 0; r < R; ++r) {
       uint32_t h[3];
