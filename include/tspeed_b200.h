@@ -224,8 +224,10 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
 
 /* Kernel variant of the batched step chosen for this handle by the
  * autotuner at creation (or forced by TSP_BATCHED_VARIANT). FP32 operator:
- * 0 K-split / pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel,
- * 2 non-persistent CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64
+ * 7 and 8 warp-specialised CUDA-core kernel with bulk-copy rings and
+ * 8-shot register tiles (packed pair FMAs / scalar FMAs), 0 K-split /
+ * pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel, 2 non-persistent
+ * CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64
  * operator with several shots: 5 warp-specialised FP64 tensor-core (DMMA)
  * kernel with two consumer groups of 8 warps (8 shots x all rows per warp),
  * 6 the same kernel with one group of 16 warps (8 shots x half the rows) and

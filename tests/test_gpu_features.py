@@ -133,7 +133,7 @@ def test_autotuner_choice_and_override(monkeypatch):
     for prec in ("fp64", "fp32"):
         with capi.Simulation.create(m.xy, m.tri, 5, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
             if prec == "fp32":
-                assert s.kernel_variant in (0, 1, 2, 4)
+                assert s.kernel_variant in (7, 8, 0, 1, 2, 4)
             if dt is None:
                 dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
             s.set_dt(dt)
@@ -182,7 +182,8 @@ def test_fp64_autotuner_choice_and_override(monkeypatch):
 @pytest.mark.parametrize("precision,op,nshots,variant", [
     ("fp64", "explicit", 1, None), ("fp64", "matrix_free", 1, None), ("fp64", "explicit", 3, "5"),
     ("fp64", "explicit", 3, "6"), ("fp64", "explicit", 3, "3"), ("fp64", "explicit", 3, "2"),
-    ("fp32", "explicit", 1, None), ("fp32", "explicit", 3, "0"), ("fp32", "explicit", 3, "4")])
+    ("fp32", "explicit", 1, None), ("fp32", "explicit", 3, "0"), ("fp32", "explicit", 3, "4"),
+    ("fp32", "explicit", 3, "7"), ("fp32", "explicit", 3, "8")])
 def test_unstable_dt_is_reported_as_nonfinite(precision, op, nshots, variant, monkeypatch):
     """A time step of 3x the CFL limit is an ordinary numerical blow-up: the
     state overflows to Inf/NaN within a few hundred steps. Every step kernel

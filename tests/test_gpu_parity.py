@@ -359,6 +359,45 @@ def test_fixed_point_tensor_core_step(N, monkeypatch):
         assert e_fx < 1e-4 and e_fx < 10 * e_simt + 1e-9
 
 
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6])
+def test_fp32_ring_kernel(N, monkeypatch):
+    """FP32-operator step on the CUDA cores with bulk-copy rings (variants 7
+    and 8), 70 shots (one full and one partial 64-shot tile), with the energy
+    monitor on: within the 1e-4 budget of the FP64 batched path shot by shot
+    and as close to it as the k-split FP32 kernel (within 10x of its error);
+    the packed pair FMAs (7) round exactly as the scalar FMAs (8), so the two
+    agree bit for bit."""
+    m = W.jittered_rect(8, 5, 800.0, 500.0, seed=N + 190)
+    rng = np.random.default_rng(N + 17)
+    vp = 2500 + 1500 * rng.random(m.ne)
+    lam, mu, rho = W.lame(vp, vp / 1.8, 2000 + 500 * rng.random(m.ne))
+    shots = [(40 + 720 * rng.random(), 40 + 420 * rng.random()) for _ in range(70)]
+    rcv = W.surface_receivers(m, 6)
+    n = 150
+    out = {}
+    dt = None
+    for tag, prec, variant in (("fp64", "fp64", "5"), ("ksplit", "fp32", "0"), ("r7", "fp32", "7"),
+                               ("r8", "fp32", "8")):
+        monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
+        with capi.Simulation.create(m.xy, m.tri, N, lam, mu, rho, shots, rcv, penalty=10.0, precision=prec) as s:
+            assert s.kernel_variant == int(variant)
+            if dt is None:
+                dt = 0.4 * 2 / np.sqrt(s.estimate_lmax(60))
+            s.set_dt(dt)
+            for k in range(70):
+                s.set_ricker(k, 25.0, 0.04, -1.0, k % 2, n)
+            s.enable_energy(True)
+            s.first_step()
+            s.run(n - 1)
+            out[tag] = (s.seismograms(0, n), s.u(3), s.u(66), s.energy(1, n - 1))
+    for i in range(4):
+        assert np.array_equal(out["r7"][i], out["r8"][i])
+    errs = [(rel(out["r7"][i], out["fp64"][i]), rel(out["ksplit"][i], out["fp64"][i])) for i in range(3)]
+    print("N", N, "(ring, k-split) vs fp64 for seismograms, u(3), u(66):", errs)
+    for e_r, e_k in errs:
+        assert e_r < 1e-4 and e_r < 10 * e_k + 1e-9
+
+
 def test_fixed_point_tensor_core_resume_and_energy(monkeypatch):
     """Variant 4: a checkpoint/resume in the middle continues bit-identically
     (the state slices are rebuilt from the FP64 state with the epilogue's own

@@ -89,7 +89,7 @@ def test_config1_full_fp64_batched(variant, monkeypatch):
         assert e_s < FP64_TOL and e_u < FP64_TOL
 
 
-@pytest.mark.parametrize("shots,variant", [([0], None), ([0, 0], 0), ([0, 0], 4)])
+@pytest.mark.parametrize("shots,variant", [([0], None), ([0, 0], 0), ([0, 0], 4), ([0, 0], 7), ([0, 0], 8)])
 def test_config1_full_fp32_operator(shots, variant, monkeypatch):
     g = load_golden("g_config1_full")
     seis, _ = run_golden(g, precision="fp32", shots=shots, monkeypatch=monkeypatch, variant=variant)
@@ -120,10 +120,11 @@ def test_config3_sample_fp64_plain_row_kernel():
         assert e_s < FP64_TOL and e_u < FP64_TOL
 
 
-@pytest.mark.parametrize("variant", [0, 4])
+@pytest.mark.parametrize("variant", [7, 8, 0, 4])
 def test_config3_sample_fp32_operator(variant, monkeypatch):
-    """FP32 operator / FP64 state: the CUDA-core kernel (0) and the
-    tensor-core fixed-point kernel (4), against the reference's FP64 run."""
+    """FP32 operator / FP64 state: the warp-specialised CUDA-core kernel
+    (7 packed pair FMAs, 8 scalar FMAs), the k-split CUDA-core kernel (0) and
+    the tensor-core fixed-point kernel (4), against the reference's FP64 run."""
     g = load_golden("g_config3_sample")
     seis, _ = run_golden(g, precision="fp32", monkeypatch=monkeypatch, variant=variant)
     e_s = seis_err(g, seis, range(len(g["src"])))

@@ -364,7 +364,8 @@ class Simulation:
     @property
     def kernel_variant(self) -> int:
         """Batched-step kernel chosen by the autotuner (or TSP_BATCHED_VARIANT):
-        FP32: 0/1/2 CUDA-core kernels, 4 tensor-core fixed-point kernel; FP64
+        FP32: 7/8 warp-specialised CUDA-core kernels with bulk-copy rings,
+        0/1/2 other CUDA-core kernels, 4 tensor-core fixed-point kernel; FP64
         with several shots: 5 and 6 warp-specialised FP64 tensor-core kernels
         (two groups of 8 consumer warps / one group of 16), 3 single-role
         one, 2 CUDA-core kernel."""

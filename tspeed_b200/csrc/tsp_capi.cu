@@ -339,8 +339,9 @@ int check_device_error(tsp_handle* h);
 // few steps on the zero initial state of the handle -- no sources are set
 // yet, so every output stays zero and nothing needs restoring -- timed with
 // CUDA events on the handle's stream; the fastest is kept. FP32 operator
-// (with its FP32 state shadow): 7 warp-specialised with bulk-copy rings and
-// 8 shots x several rows per lane, 0 K split over warp groups, 1 pipelined
+// (with its FP32 state shadow): 7 and 8 warp-specialised with bulk-copy rings
+// and 8 shots x several rows per lane (packed pair FMAs / scalar FMAs), 0 K
+// split over warp groups, 1 pipelined
 // single group, 2 non-persistent, 4 tensor-core fixed point. FP64 operator: 5 and 6
 // warp-specialised DMMA (two consumer groups of 8 warps, or one group of 16
 // warps with a latency-free epilogue), 3 single-role DMMA, 2 CUDA cores. TSP_BATCHED_VARIANT skips
@@ -372,8 +373,8 @@ int autotune(tsp_handle* h) {
   }
   std::vector<int> cands;
   if (fp64_batched) cands = {5, 6, 3, 2};
-  else if (h->R <= 42) cands = {7, 0, 1, 2};
-  else if (h->R <= 56) cands = {7, 0, 2};
+  else if (h->R <= 42) cands = {7, 8, 0, 1, 2};
+  else if (h->R <= 56) cands = {7, 8, 0, 2};
   else cands = {2};
   if (fx_ok) cands.push_back(4);
   if (cached >= 0 && (cached != 4 || fx_ok)) cands = {cached};
@@ -640,7 +641,7 @@ int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 // a ring per group. Seven warps per CTA leave each thread up to 255
 // registers: the 8-shot x RL-row tiles and the FP64 epilogue fit without
 // spills (nine warps cap a thread at 168 registers and spill).
-template <int R>
+template <int R, int F2>
 int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   constexpr int NWG = tsp::S32WCfg<R>::NWG;
   constexpr int NGR = 6 / NWG;
@@ -651,14 +652,14 @@ int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   static unsigned long long configured = 0;
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG>,
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG, F2>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP32 ring kernel smem: ") + cudaGetErrorString(e));
     configured |= bit;
   }
   const long long items = (long long)h->ne * ((h->S + 63) / 64);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
-  tsp::k_step_batched32w<R, NGR, NSG><<<grid, LY::NT, smem, st>>>(p, h->d_err);
+  tsp::k_step_batched32w<R, NGR, NSG, F2><<<grid, LY::NT, smem, st>>>(p, h->d_err);
   return TSP_OK;
 }
 
@@ -685,8 +686,9 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   if constexpr (R <= 56) {
     if (h->fx && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) return launch_fx<R>(h, p, st);
   }
-  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant == 7) {
-    if constexpr (R <= 56) return launch_s32w<R>(h, p, st);
+  if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) &&
+      (h->kernel_variant == 7 || h->kernel_variant == 8)) {
+    if constexpr (R <= 56) return h->kernel_variant == 7 ? launch_s32w<R, 1>(h, p, st) : launch_s32w<R, 0>(h, p, st);
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 42) {

@@ -77,7 +77,26 @@ constexpr int s32w_fit_nsg() {
   return int(budget / one) >= 6 ? 6 : int(budget / one);
 }
 
-template <int R, int NGR, int NSG>
+// Packed FP32 FMA on pairs (Blackwell fma.rn.f32x2: each half rounds exactly
+// as fmaf does, so results are bit-identical; one instruction per two FMAs
+// leaves issue slots to the loads).
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f32x2_splat(float v) {
+  unsigned long long d;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(d) : "f"(v));
+  return d;
+}
+__device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+// F2 selects packed pair FMAs (1) or scalar FMAs (0) for the products.
+template <int R, int NGR, int NSG, int F2>
 __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
     k_step_batched32w(const StepParams p, int* err_flag) {
   typedef S32WCfg<R> CF;
@@ -169,10 +188,14 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
       const int s0 = tile * ST;
       const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
       float acc[RL][8];
+      unsigned long long acc2[RL][4];  // F2: shots (2m, 2m + 1) of the lane's 8
 #pragma unroll
-      for (int i = 0; i < RL; ++i)
+      for (int i = 0; i < RL; ++i) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) acc[i][q] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) acc2[i][m] = 0ull;
+      }
       for (int b = 0; b < nb; ++b) {
         const int s = int(j % NSG);
         const uint32_t n = j / NSG;
@@ -187,9 +210,6 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
         const float* Xs = gst + size_t(s) * CF::STAGE + CF::BSZ + 4 * sg;
 #pragma unroll 2
         for (int kk = 0; kk < R; ++kk) {
-          const float4 xa = *reinterpret_cast<const float4*>(Xs + kk * ST);
-          const float4 xb = *reinterpret_cast<const float4*>(Xs + kk * ST + 32);
-          const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
           float bv[RL];
 #pragma unroll
           for (int i = 0; i < RL; i += 2) {
@@ -197,13 +217,34 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
             bv[i] = b2.x;
             bv[i + 1] = b2.y;
           }
+          if constexpr (F2) {
+            const ulonglong2 xa = *reinterpret_cast<const ulonglong2*>(Xs + kk * ST);
+            const ulonglong2 xb = *reinterpret_cast<const ulonglong2*>(Xs + kk * ST + 32);
+            const unsigned long long xp[4] = {xa.x, xa.y, xb.x, xb.y};
 #pragma unroll
-          for (int i = 0; i < RL; ++i)
+            for (int i = 0; i < RL; ++i) {
+              const unsigned long long bb = f32x2_splat(bv[i]);
 #pragma unroll
-            for (int q = 0; q < 8; ++q) acc[i][q] = fmaf(xv[q], bv[i], acc[i][q]);
+              for (int m = 0; m < 4; ++m) acc2[i][m] = ffma2(xp[m], bb, acc2[i][m]);
+            }
+          } else {
+            const float4 xa = *reinterpret_cast<const float4*>(Xs + kk * ST);
+            const float4 xb = *reinterpret_cast<const float4*>(Xs + kk * ST + 32);
+            const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+#pragma unroll
+            for (int i = 0; i < RL; ++i)
+#pragma unroll
+              for (int q = 0; q < 8; ++q) acc[i][q] = fmaf(xv[q], bv[i], acc[i][q]);
+          }
         }
         __syncwarp();
         if (lane == 0) fx_mbar_arrive(smem_u32(&gempty[s]));
+      }
+      if constexpr (F2) {
+#pragma unroll
+        for (int i = 0; i < RL; ++i)
+#pragma unroll
+          for (int m = 0; m < 4; ++m) f32x2_unpack(acc2[i][m], acc[i][2 * m], acc[i][2 * m + 1]);
       }
       // ---- epilogue (FP64 leap-frog, source, energy; FP32 shadow) ----
       const size_t tix = size_t(e) * ntile + tile;
