@@ -291,11 +291,17 @@ def errors_vs_reference():
                             ("batched_fp32_cuda_core", "fp32", 0)):
         seis, v = run_on_golden(g, prec, list(range(ns)), var)
         out["forms"][name] = {"err": err(seis, ref), "kernel_variant": v}
+    # The single-shot drop-in runs shot by shot; a deep source's traces are
+    # orders of magnitude weaker than the shallow ones' (its wavefront has
+    # barely reached the surface), so each shot's trace error is measured
+    # against the whole gather's norm, as the batched forms' errors are.
     errs = []
+    gather = float(np.linalg.norm(ref))
     for k in (0, ns - 1):
         seis, _ = run_on_golden(g, "fp64", [k])
-        errs.append(err(seis[0], ref[k]))
-    out["forms"]["plain_fp64_single_shot"] = {"err": max(errs), "shots_checked": [0, ns - 1]}
+        errs.append(float(np.linalg.norm(seis[0] - ref[k])) / gather)
+    out["forms"]["plain_fp64_single_shot"] = {"err": max(errs), "shots_checked": [0, ns - 1],
+                                              "normalised_by": "norm of the 8-shot gather"}
     return out
 
 
@@ -308,7 +314,7 @@ def energy_drift(prob, dt, nsteps=500):
     out = {"steps": nsteps, "initial_field": "Gaussian pulse of u_y (sigma 150 m) at each source point",
            "forms": {}}
     for name, prec, nsh in (("batched_fp64", "fp64", prob.nshots), ("batched_fp32_operator", "fp32", prob.nshots),
-                            ("plain_fp64_single_shot", "fp64", 1)):
+                            ("plain_fp64_single_shot", "fp64", 1), ("plain_fp32_operator_single_shot", "fp32", 1)):
         with capi.Simulation.create(prob.mesh.xy, prob.mesh.tri, prob.N, prob.lam, prob.mu, prob.rho,
                                     [(sr.x, sr.y) for sr in prob.sources[:nsh]], [], penalty=prob.penalty,
                                     precision=prec) as s:

@@ -111,13 +111,27 @@ def test_config3_sample_fp64_batched(variant, monkeypatch):
 
 
 def test_config3_sample_fp64_plain_row_kernel():
-    """The single-shot drop-in (row kernel), shot by shot."""
+    """The single-shot drop-in (row kernel), shot by shot: the final
+    displacement within 1e-12, and the receiver traces within 1e-12 of the
+    gather's scale. A deep source's wavefront has barely reached the surface
+    after 3,000 steps (shot 0: its traces are 2e4 times weaker than the
+    shallow shots'); rounding differences of summation order are set by the
+    field's magnitude, not by those weak traces, so traces are measured
+    against the norm of the whole 8-shot gather, as the batched tests do.
+    A shot with strong arrivals (3) is also held to 1e-12 of its own traces."""
     g = load_golden("g_config3_sample")
+    every = int(g["seis_every"])
+    gather = np.linalg.norm(g["seis"])
     for i, k in enumerate(g["u_shots"]):
         seis, us = run_golden(g, shots=[int(k)])
-        e_s, e_u = seis_err(g, seis, [int(k)]), rel(us[0], g["u_final"][i])
-        print("shot", int(k), "seismograms", e_s, "u", e_u)
+        e_s = float(np.linalg.norm(seis[0, ::every] - g["seis"][int(k)]) / gather)
+        e_u = rel(us[0], g["u_final"][i])
+        print("shot", int(k), "seismograms (of the gather)", e_s, "u", e_u)
         assert e_s < FP64_TOL and e_u < FP64_TOL
+    seis, _ = run_golden(g, shots=[3])
+    e3 = seis_err(g, seis, [3])
+    print("shot 3 seismograms", e3)
+    assert e3 < FP64_TOL
 
 
 @pytest.mark.parametrize("variant", [7, 8, 0, 4])
