@@ -56,8 +56,10 @@ def test_noalloc_lmax_matches_allocating_entry_point(N, precision, op, nshots):
     # Same power iteration from another start vector: both converge to lmax.
     assert abs(first - ref) / ref < 1e-6
     assert abs(second - ref) / ref < 1e-6
-    # The shared scratch is re-initialised by every call.
-    assert second == first
+    # The shared scratch is re-initialised by every call: the second call
+    # repeats the first, up to the order in which the device's atomic sums
+    # of the Rayleigh quotient land (last bits).
+    assert abs(second - first) <= 1e-12 * abs(first)
 
 
 def test_noalloc_rejects_problems_beyond_the_scratch():

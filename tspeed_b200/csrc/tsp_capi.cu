@@ -637,29 +637,29 @@ int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 // FP32-operator step on the CUDA cores with warp-specialised bulk-copy rings
-// (variant 7): 6 consumer warps in groups of NWG (one or two warps per item),
-// a ring per group. Seven warps per CTA leave each thread up to 255
-// registers: the 8-shot x RL-row tiles and the FP64 epilogue fit without
-// spills (nine warps cap a thread at 168 registers and spill).
+// (variants 7 and 8: packed pair FMAs / scalar FMAs): pairs of an FMA group
+// (NWG warps per item) and an update set of 2 warps (the FP64 epilogue), a
+// ring and a Y tile per pair; 6 FMA warps in all (3 pairs at 2Np = 42).
 template <int R, int F2>
 int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   constexpr int NWG = tsp::S32WCfg<R>::NWG;
-  constexpr int NGR = 6 / NWG;
-  constexpr int NSG = tsp::s32w_fit_nsg<R, NGR>();
-  static_assert(NSG >= 2, "FP32 ring: two stages per group must fit");
-  typedef tsp::S32WLayout<R, NGR, NSG> LY;
+  constexpr int NGR = NWG == 1 ? 4 : 3;
+  constexpr int NU = 2;
+  constexpr int NSG = tsp::s32w_fit_nsg<R, NGR, NU>();
+  static_assert(NSG >= 2, "FP32 ring: two stages per pair must fit");
+  typedef tsp::S32WLayout<R, NGR, NSG, NU> LY;
   const size_t smem = LY::smem_bytes();
   static unsigned long long configured = 0;
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG, F2>,
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG, NU, F2>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP32 ring kernel smem: ") + cudaGetErrorString(e));
     configured |= bit;
   }
   const long long items = (long long)h->ne * ((h->S + 63) / 64);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
-  tsp::k_step_batched32w<R, NGR, NSG, F2><<<grid, LY::NT, smem, st>>>(p, h->d_err);
+  tsp::k_step_batched32w<R, NGR, NSG, NU, F2><<<grid, LY::NT, smem, st>>>(p, h->d_err);
   return TSP_OK;
 }
 

@@ -12,25 +12,33 @@
 // FP64 (u^k, u^{k-1} and u^{k+1} in FP64); the epilogue also writes the FP32
 // shadow of u^{k+1} that the next step's neighbours read.
 //
-// Data flow: one producer lane per consumer group streams, per block, two
-// bulk copies into the group's own ring of NSG stages (cp.async.bulk,
-// completion on mbarriers, no multicast): the stored FP32 block (column-major,
-// pitch KP = 2Np padded to 4) and the neighbour's FP32 shadow tile (2Np rows
-// of 64 shots, contiguous). A ring per group makes every mbarrier wait
-// unambiguous (index j - NSG of a ring is always its own group's consumed
-// block). NGR groups of NWG warps take the CTA's items in turn, so one
-// group's epilogue (FP64 global loads and stores) overlaps the others'
-// products.
+// Roles: NGR pairs of an FMA group (NWG warps: the products of one item) and
+// an update set (NU warps: the FP64 epilogue of that group's items), and a
+// producer warp. One producer lane per pair streams, per block, two bulk
+// copies into the pair's own ring of NSG stages (cp.async.bulk, completion
+// on mbarriers, no multicast): the stored FP32 block (column-major, pitch
+// KP = 2Np padded to 4) and the neighbour's FP32 shadow tile (2Np rows of
+// 64 shots, contiguous). The FMA group writes the item's FP32 row sums into
+// the pair's Y tile in shared memory and goes on with its next item; the
+// update set reads them, runs the leap-frog update with coalesced FP64 loads
+// and stores of the contiguous state tile (a shot tile of an element is one
+// run of 64 x 2Np doubles), writes u^{k+1} back into the Y tile in FP32 and
+// stores it transposed as the next step's shadow (rows of 64 shots,
+// coalesced), then samples the receivers. The FMA warps never wait on global
+// memory; the update sets hide their load latency behind the products.
+// Every ring and the Y tile are used by one pair only, in its own item
+// order, so each mbarrier wait is unambiguous (use n - 1 of a barrier is
+// always one the waiter consumed itself).
 //
-// Lane (sg, rg) of warp w of a group: shots 4 sg .. 4 sg + 3 and
+// Lane (sg, rg) of warp w of an FMA group: shots 4 sg .. 4 sg + 3 and
 // 32 + 4 sg .. 32 + 4 sg + 3 (each quarter-warp reads 128 contiguous bytes
 // of a state row: conflict-free), rows w RW + rg RL .. + RL - 1 with
 // RW = 4 RL. Rows at or beyond 2Np (the last warp's padding) are computed
 // from in-bounds shared memory (the stage's tail) and never stored.
 //
 // Every wait is bounded (about a second); on a timeout the CTA raises an
-// abort flag in shared memory, every role stops waiting, the consumer warps
-// keep their named barriers balanced, the producers wait (bounded) for their
+// abort flag in shared memory, every role stops waiting, the update sets keep
+// their named barriers balanced, the producers wait (bounded) for their
 // copies in flight, and err_flag tells the host that the results are void.
 #pragma once
 
@@ -59,27 +67,34 @@ struct S32WCfg {
   static_assert((R - 1) * KP + NWG * RW <= STAGE, "padding rows stay inside the stage");
 };
 
-template <int R, int NGR, int NSG>
+template <int R, int NGR, int NSG, int NU>
 struct S32WLayout {
   typedef S32WCfg<R> C;
-  static constexpr int NT = (NGR * C::NWG + 1) * 32;
+  static constexpr int NF = NGR * C::NWG;              // FMA warps
+  static constexpr int NUT = NU * 32;                  // threads of an update set
+  static constexpr int NT = (NF + NGR * NU + 1) * 32;  // + update warps + the producer warp
   static constexpr int NST = NGR * NSG;
+  static constexpr int YP = R + 1;                     // odd pitch of the Y tile [shot][YP]
+  static constexpr int YSZ = C::ST * YP;               // floats of one pair's Y tile
+  static_assert((YSZ * 4) % 16 == 0, "aligned barriers after the Y tiles");
   static constexpr size_t smem_bytes() {
-    return size_t(NST) * C::STAGE * sizeof(float) + size_t(2 * NST) * sizeof(uint64_t) + 16;
+    return size_t(NST) * C::STAGE * sizeof(float) + size_t(NGR) * YSZ * sizeof(float) +
+           size_t(2 * NST + 2 * NGR) * sizeof(uint64_t) + 16;
   }
 };
 
-// Groups x stages per group that fit in shared memory.
-template <int R, int NGR>
+// Stages per pair ring that fit in shared memory beside the Y tiles.
+template <int R, int NGR, int NU>
 constexpr int s32w_fit_nsg() {
-  constexpr size_t one = S32WLayout<R, NGR, 1>::smem_bytes();
+  typedef S32WLayout<R, NGR, 1, NU> L1;
+  constexpr size_t fixed = L1::smem_bytes() - size_t(NGR) * S32WCfg<R>::STAGE * sizeof(float);
+  constexpr size_t per = size_t(NGR) * (S32WCfg<R>::STAGE * sizeof(float) + 2 * sizeof(uint64_t));
   constexpr size_t budget = 227 * 1024;
-  return int(budget / one) >= 6 ? 6 : int(budget / one);
+  return int((budget - fixed) / per) >= 6 ? 6 : int((budget - fixed) / per);
 }
 
-// Packed FP32 FMA on pairs (Blackwell fma.rn.f32x2: each half rounds exactly
-// as fmaf does, so results are bit-identical; one instruction per two FMAs
-// leaves issue slots to the loads).
+// Packed FP32 FMA on pairs (Blackwell fma.rn.f32x2; one instruction per two
+// FMAs leaves issue slots to the loads).
 __device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
                                                     unsigned long long c) {
   unsigned long long d;
@@ -96,18 +111,21 @@ __device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, fl
 }
 
 // F2 selects packed pair FMAs (1) or scalar FMAs (0) for the products.
-template <int R, int NGR, int NSG, int F2>
-__global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
+template <int R, int NGR, int NSG, int NU, int F2>
+__global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
     k_step_batched32w(const StepParams p, int* err_flag) {
   typedef S32WCfg<R> CF;
-  typedef S32WLayout<R, NGR, NSG> LY;
+  typedef S32WLayout<R, NGR, NSG, NU> LY;
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, RL = CF::RL, RW = CF::RW, NWG = CF::NWG;
-  constexpr int NST = LY::NST;
+  constexpr int NST = LY::NST, NF = LY::NF, NUT = LY::NUT, YP = LY::YP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* stages = reinterpret_cast<float*>(smem_raw);
-  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NGR][NSG] stage landed
+  float* ybuf = stages + size_t(NST) * CF::STAGE;                                    // [NGR][ST][YP]
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(ybuf + size_t(NGR) * LY::YSZ);      // [NGR][NSG] stage landed
   uint64_t* bempty = bfull + NST;                                                    // [NGR][NSG] stage consumed
-  volatile int* abort_s = reinterpret_cast<volatile int*>(bempty + NST);
+  uint64_t* yfull = bempty + NST;                                                    // [NGR] Y tile written
+  uint64_t* yempty = yfull + NGR;                                                    // [NGR] Y tile consumed
+  volatile int* abort_s = reinterpret_cast<volatile int*>(yempty + NGR);
 
   if (*reinterpret_cast<volatile int*>(err_flag) != 0) return;  // an earlier launch of the run timed out
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -117,9 +135,13 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
       fx_mbar_init(smem_u32(&bfull[i]), 1);
       fx_mbar_init(smem_u32(&bempty[i]), NWG);
     }
+    for (int i = 0; i < NGR; ++i) {
+      fx_mbar_init(smem_u32(&yfull[i]), NWG);
+      fx_mbar_init(smem_u32(&yempty[i]), NU);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = t; i < NST * CF::STAGE; i += LY::NT) stages[i] = 0.0f;
+  for (int i = t; i < NST * CF::STAGE + NGR * LY::YSZ; i += LY::NT) stages[i] = 0.0f;
   __syncthreads();
 
   const int S = p.S;
@@ -128,7 +150,7 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
   const long long G = gridDim.x;
   const float* blocks = reinterpret_cast<const float*>(p.blocks);
 
-  if (warp == NGR * NWG) {
+  if (warp == NF + NGR * NU) {
     // ---------------- producers: lane g fills ring g ----------------
     if (lane < NGR) {
       const int g = lane;
@@ -168,24 +190,21 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
       }
       if (clock64() - t0 >= (1ll << 31)) *abort_s = 1;
     }
-  } else {
-    // ---------------- consumers ----------------
-    const int grp = warp / NWG, w = warp % NWG, tl = t - grp * NWG * 32;
+  } else if (warp < NF) {
+    // ---------------- FMA groups ----------------
+    const int grp = warp / NWG, w = warp % NWG;
     const int sg = lane & 7, rg = lane >> 3;
     const int rbase = w * RW + rg * RL;  // the lane's first row
-    const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
-    const double dt = p.dt;
     uint64_t* gfull = bfull + grp * NSG;
     uint64_t* gempty = bempty + grp * NSG;
     const float* gst = stages + size_t(grp) * NSG * CF::STAGE;
-    double en = 0.0;
-    uint32_t j = 0;  // index into this group's ring
+    float* Y = ybuf + size_t(grp) * LY::YSZ;
+    uint32_t j = 0, m = 0;  // ring index; uses of the Y tile
     bool dead = false;
     long long it = 0;
     for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
-      if (int(it % NGR) != grp) continue;  // another group's item (its own ring)
-      const int e = int(item / ntile), tile = int(item % ntile);
-      const int s0 = tile * ST;
+      if (int(it % NGR) != grp) continue;  // another pair's item
+      const int e = int(item / ntile);
       const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
       float acc[RL][8];
       unsigned long long acc2[RL][4];  // F2: shots (2m, 2m + 1) of the lane's 8
@@ -194,7 +213,7 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
 #pragma unroll
         for (int q = 0; q < 8; ++q) acc[i][q] = 0.0f;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) acc2[i][m] = 0ull;
+        for (int mm = 0; mm < 4; ++mm) acc2[i][mm] = 0ull;
       }
       for (int b = 0; b < nb; ++b) {
         const int s = int(j % NSG);
@@ -225,7 +244,7 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
             for (int i = 0; i < RL; ++i) {
               const unsigned long long bb = f32x2_splat(bv[i]);
 #pragma unroll
-              for (int m = 0; m < 4; ++m) acc2[i][m] = ffma2(xp[m], bb, acc2[i][m]);
+              for (int mm = 0; mm < 4; ++mm) acc2[i][mm] = ffma2(xp[mm], bb, acc2[i][mm]);
             }
           } else {
             const float4 xa = *reinterpret_cast<const float4*>(Xs + kk * ST);
@@ -244,97 +263,117 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG>::NT, 1)
 #pragma unroll
         for (int i = 0; i < RL; ++i)
 #pragma unroll
-          for (int m = 0; m < 4; ++m) f32x2_unpack(acc2[i][m], acc[i][2 * m], acc[i][2 * m + 1]);
+          for (int mm = 0; mm < 4; ++mm) f32x2_unpack(acc2[i][mm], acc[i][2 * mm], acc[i][2 * mm + 1]);
       }
-      // ---- epilogue (FP64 leap-frog, source, energy; FP32 shadow) ----
+      // ---- hand the row sums to the pair's update set ----
+      if (!dead && m > 0) {
+        const bool okw = fx_wait(smem_u32(&yempty[grp]), (m - 1) & 1, abort_s);
+        if (__any_sync(0xffffffffu, !okw)) dead = true;
+      }
+      ++m;
+      if (dead) continue;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int sl = (q < 4 ? 0 : 32) + 4 * sg + (q & 3);
+#pragma unroll
+        for (int i = 0; i < RL; ++i)
+          if (rbase + i < R) Y[sl * YP + rbase + i] = acc[i][q];
+      }
+      __syncwarp();
+      if (lane == 0) fx_mbar_arrive(smem_u32(&yfull[grp]));
+    }
+  } else {
+    // ---------------- update sets: FP64 epilogue of the pair's items ----------------
+    const int ug = (warp - NF) / NU;
+    const int ut = t - (NF + ug * NU) * 32;  // thread within the set
+    const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+    const double dt = p.dt;
+    float* Y = ybuf + size_t(ug) * LY::YSZ;
+    constexpr int BATCH = 6;  // row pairs per thread and load batch
+    double en = 0.0;
+    uint32_t m = 0;
+    bool dead = false;
+    long long it = 0;
+    for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
+      if (int(it % NGR) != ug) continue;
+      const int e = int(item / ntile), tile = int(item % ntile);
+      const int s0 = tile * ST, nsv = min(ST, S - s0);
+      const size_t base = (size_t(e) * S + s0) * R;  // the tile: nsv * R contiguous doubles
       const size_t tix = size_t(e) * ntile + tile;
       if (!dead) {
+        const bool okw = fx_wait(smem_u32(&yfull[ug]), m & 1, abort_s);
+        if (!__all_sync(0xffffffffu, okw)) dead = true;
+      }
+      ++m;
+      if (!dead) {
         const double mi = p.minv[e];
+        const int npair = nsv * NP;
+        for (int pb = 0; pb < npair; pb += NUT * BATCH) {
+          // Row pair q = pb + NUT b + ut is entry 2q of the tile: shot q / NP,
+          // rows 2 (q % NP) and +1. Both levels' loads first (coalesced).
+          double2 uu[BATCH], up[BATCH];
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          // Shots 32 half + 4 sg + q, q < 4; their source terms first.
-          bool src[4];
-          double Fk[4][2];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int sh = s0 + 32 * half + 4 * sg + q;
-            src[q] = sh < S && (p.src_elem[sh] == e) && (k < p.nF);
-            Fk[q][0] = src[q] ? p.F[(size_t(sh) * p.nF + k) * 2] : 0.0;
-            Fk[q][1] = src[q] ? p.F[(size_t(sh) * p.nF + k) * 2 + 1] : 0.0;
+          for (int b = 0; b < BATCH; ++b) {
+            const int q = pb + NUT * b + ut;
+            const bool v = q < npair;
+            uu[b] = v ? __ldg(reinterpret_cast<const double2*>(p.x + base) + q) : make_double2(0.0, 0.0);
+            up[b] = (v && p.uprev) ? *(reinterpret_cast<const double2*>(p.uprev + base) + q) : make_double2(0.0, 0.0);
           }
-          float sv[RL][4];
 #pragma unroll
-          for (int i = 0; i < RL / 2; ++i) {
-            // Row pair rbase + 2i of the four shots: both levels' loads first.
-            const int r0 = rbase + 2 * i;
-            double2 uu[4], up[4];
+          for (int b = 0; b < BATCH; ++b) {
+            const int q = pb + NUT * b + ut;
+            if (q >= npair) continue;
+            const int sl = q / NP, r0 = 2 * (q - sl * NP);
+            const int sh = s0 + sl;
+            const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+            const double u[2] = {uu[b].x, uu[b].y}, upr[2] = {up[b].x, up[b].y};
+            double un[2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int sh = s0 + 32 * half + 4 * sg + q;
-              const bool v = sh < S && r0 < R;
-              const size_t me = (size_t(e) * S + (v ? sh : 0)) * R + (v ? r0 : 0);
-              uu[q] = v ? __ldg(reinterpret_cast<const double2*>(p.x + me)) : make_double2(0.0, 0.0);
-              up[q] = (v && p.uprev) ? *reinterpret_cast<const double2*>(p.uprev + me) : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int sh = s0 + 32 * half + 4 * sg + q;
-              const bool v = sh < S && r0 < R;
-              const double u[2] = {uu[q].x, uu[q].y}, upr[2] = {up[q].x, up[q].y};
-              double un[2];
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int r = r0 + h;
-                const int cmp = r / NP, ii = r - cmp * NP;
-                const double f = (src[q] && r < R) ? Fk[q][cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
-                const double y = double(acc[2 * i + h][4 * half + q]);
-                if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
-                else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
-                if (p.energy != nullptr && v) {
-                  const double d = un[h] - u[h];
-                  en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
-                }
-                sv[2 * i + h][q] = v ? float(un[h]) : 0.0f;
+            for (int h = 0; h < 2; ++h) {
+              const int r = r0 + h;
+              const int cmp = r / NP, ii = r - cmp * NP;
+              const double f = is_src ? p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+              const double y = double(Y[sl * YP + r]);
+              if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
+              else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+              if (p.energy != nullptr) {
+                const double d = un[h] - u[h];
+                en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
               }
-              if (v) {
-                *reinterpret_cast<double2*>(p.out + (size_t(e) * S + sh) * R + r0) = make_double2(un[0], un[1]);
-                note_nonfinite(p, un[0], un[1]);
-              }
+              Y[sl * YP + r] = float(un[h]);
             }
-          }
-          // FP32 shadow of u^{k+1}: row r, shots 32 half + 4 sg .. + 3 (one
-          // 16-byte store; the 8 lanes of a row group write 128 bytes).
-#pragma unroll
-          for (int i = 0; i < RL; ++i) {
-            const int r = rbase + i;
-            if (r < R)
-              *reinterpret_cast<float4*>(p.x32_out + (tix * R + r) * ST + 32 * half + 4 * sg) =
-                  make_float4(sv[i][0], sv[i][1], sv[i][2], sv[i][3]);
+            *(reinterpret_cast<double2*>(p.out + base) + q) = make_double2(un[0], un[1]);
+            note_nonfinite(p, un[0], un[1]);
           }
         }
       }
-      // ---- receivers (the condition is the same for every warp of the group) ----
-      if (p.rcv_ptr != nullptr) {
-        const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
-        if (q1 > q0) {
-          // u^{k+1} of this item is visible to the whole group (barrier 1 + grp).
-          asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(NWG * 32) : "memory");
-          if (!dead) {
-            const long long slot = k % p.seis_cap;
-            const int nwork = (q1 - q0) * ST * 2;
-            for (int wk = tl; wk < nwork; wk += NWG * 32) {
-              const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
-              const int sh = s0 + sl;
-              if (sh >= S) continue;
-              const int rid = p.rcv_id[q];
-              const double* ph = p.rcv_phi + size_t(rid) * NP;
-              const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
-              double v = 0.0;
-              for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
-              p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
-            }
+      // u^{k+1} of the item (FP64 in global memory, FP32 in the Y tile) is
+      // complete once the whole set passes this barrier (id 1 + pair).
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + ug), "n"(NUT) : "memory");
+      if (!dead) {
+        // FP32 shadow of u^{k+1}, transposed: rows of 64 shots (shots beyond
+        // S stay zero), 32 consecutive floats per warp store.
+        for (int idx = ut; idx < R * ST; idx += NUT) {
+          const int r = idx / ST, sl = idx - r * ST;
+          p.x32_out[(tix * R + r) * ST + sl] = sl < nsv ? Y[sl * YP + r] : 0.0f;
+        }
+        // Receivers of this element.
+        if (p.rcv_ptr != nullptr) {
+          const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+          const long long slot = k % p.seis_cap;
+          for (int wk = ut; wk < (q1 - q0) * nsv * 2; wk += NUT) {
+            const int cmp = wk & 1, sl = (wk >> 1) % nsv, q = q0 + (wk >> 1) / nsv;
+            const int sh = s0 + sl;
+            const int rid = p.rcv_id[q];
+            const double* ph = p.rcv_phi + size_t(rid) * NP;
+            const double* un = p.out + base + size_t(sl) * R + cmp * NP;
+            double v = 0.0;
+            for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+            p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
           }
         }
+        __syncwarp();
+        if (lane == 0) fx_mbar_arrive(smem_u32(&yempty[ug]));
       }
     }
     if (p.energy != nullptr) {
