@@ -160,28 +160,29 @@ def test_fp64_autotuner_choice_and_override(monkeypatch):
     rcv = W.surface_receivers(m, 4)
     n = 40
     out = {}
-    for forced in (None, "5", "6", "3", "2"):
+    for forced in (None, "5", "6", "9", "10", "3", "2"):
         if forced is None:
             monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
         else:
             monkeypatch.setenv("TSP_BATCHED_VARIANT", forced)
         with capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, shots, rcv, penalty=10.0) as s:
             v = s.kernel_variant
-            assert v in (5, 6, 3, 2) if forced is None else v == int(forced)
+            assert v in (5, 6, 9, 10, 3, 2) if forced is None else v == int(forced)
             s.set_dt(2e-4)
             for k in range(len(shots)):
                 s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)
             s.first_step()
             s.run(n - 1)
             out[forced] = s.seismograms(0, n)
-    for forced in ("5", "6", "3"):
+    for forced in ("5", "6", "9", "10", "3"):
         assert np.linalg.norm(out[forced] - out["2"]) <= 1e-13 * np.linalg.norm(out["2"])
     assert np.linalg.norm(out[None] - out["2"]) <= 1e-13 * np.linalg.norm(out["2"])
 
 
 @pytest.mark.parametrize("precision,op,nshots,variant", [
     ("fp64", "explicit", 1, None), ("fp64", "matrix_free", 1, None), ("fp64", "explicit", 3, "5"),
-    ("fp64", "explicit", 3, "6"), ("fp64", "explicit", 3, "3"), ("fp64", "explicit", 3, "2"),
+    ("fp64", "explicit", 3, "6"), ("fp64", "explicit", 3, "9"), ("fp64", "explicit", 3, "10"),
+    ("fp64", "explicit", 3, "3"), ("fp64", "explicit", 3, "2"),
     ("fp32", "explicit", 1, None), ("fp32", "explicit", 3, "0"), ("fp32", "explicit", 3, "4"),
     ("fp32", "explicit", 3, "7"), ("fp32", "explicit", 3, "8")])
 def test_unstable_dt_is_reported_as_nonfinite(precision, op, nshots, variant, monkeypatch):

@@ -357,7 +357,8 @@ int autotune(tsp_handle* h) {
   const bool fp64_batched = h->S > 1 && h->prec == TSP_PREC_FP64 && h->op_kind == TSP_OP_EXPLICIT;
   if (fp64_batched) {
     if (h->kernel_variant >= 0) {
-      if (h->kernel_variant != 2 && h->kernel_variant != 3 && h->kernel_variant != 6) h->kernel_variant = 5;
+      const int v = h->kernel_variant;
+      if (v != 2 && v != 3 && v != 6 && v != 9 && v != 10) h->kernel_variant = 5;
       return TSP_OK;
     }
   } else if (h->kernel_variant >= 0 || !h->shadow) {
@@ -372,7 +373,7 @@ int autotune(tsp_handle* h) {
     if (it != g_tune_cache.end()) cached = it->second;
   }
   std::vector<int> cands;
-  if (fp64_batched) cands = {5, 6, 3, 2};
+  if (fp64_batched) cands = {5, 9, 10, 6, 3, 2};
   else if (h->R <= 42) cands = {7, 8, 0, 1, 2};
   else if (h->R <= 56) cands = {7, 8, 0, 2};
   else cands = {2};
@@ -564,6 +565,37 @@ int launch_d64w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   return TSP_OK;
 }
 
+// FP64 warp-specialised DMMA step with the decoupled epilogue (EPI = 2):
+// V = 9, two groups of 8 DMMA warps (8 shots x all rows per warp), one
+// update warp and a 2-stage ring per group; V = 10, one group of 16 DMMA
+// warps (8 shots x half the rows), two update warps and a 5-stage ring.
+// The DMMA warps hand their FP64 row sums to the update warps through a Y
+// tile in shared memory and never wait on global memory.
+template <int R, int V>
+int launch_d64u(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
+  constexpr int NG = (V == 9 && R <= 56) ? 2 : 1;
+  constexpr int ST = tsp::D64WCfg<R, 1, NG>::ST;
+  constexpr int NCW = (V == 9) ? 8 : 16;
+  constexpr int WM = ST / 8, WN = NCW / WM;
+  constexpr int NU = (V == 9) ? 1 : 2;
+  constexpr int NSG = tsp::d64w_fit_nsg_upd<R, NG, WM, WN, NU, (NG == 1 ? 6 : 4)>();
+  static_assert(NSG >= 2, "FP64 DMMA ring: two stages per group must fit");
+  typedef tsp::D64WUpd<R, NSG, NG, WM, WN, NU> UF;
+  const size_t smem = UF::smem_bytes();
+  static unsigned long long configured = 0;  // one bit per device
+  const unsigned long long bit = 1ull << (h->device & 63);
+  if (!(configured & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, 2, NU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP64 batched kernel smem: ") + cudaGetErrorString(e));
+    configured |= bit;
+  }
+  const long long items = (long long)h->ne * ((h->S + ST - 1) / ST);
+  const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
+  tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, 2, NU><<<grid, UF::NT, smem, st>>>(p, h->d_err);
+  return TSP_OK;
+}
+
 template <int N>
 int launch_matfree_N(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   typedef tsp::MFCfg<N> CF;
@@ -719,9 +751,11 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   // register-staged CUDA-core kernel.
   if (h->S > 1 && h->prec == TSP_PREC_FP64 && h->kernel_variant != 2 &&
       (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
-    return h->kernel_variant == 3 ? launch_d64<R>(h, p, st)
-           : h->kernel_variant == 6 ? launch_d64w<R, 6>(h, p, st)
-                                    : launch_d64w<R, 5>(h, p, st);
+    return h->kernel_variant == 3    ? launch_d64<R>(h, p, st)
+           : h->kernel_variant == 6  ? launch_d64w<R, 6>(h, p, st)
+           : h->kernel_variant == 9  ? launch_d64u<R, 9>(h, p, st)
+           : h->kernel_variant == 10 ? launch_d64u<R, 10>(h, p, st)
+                                     : launch_d64w<R, 5>(h, p, st);
   if (h->S > 1 && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst)) {
     typedef tsp::BatchCfg<R> CF;
     const dim3 grid(unsigned(h->ne), unsigned((h->S + CF::ST - 1) / CF::ST));

@@ -81,23 +81,57 @@ constexpr int d64w_fit_nsg() {
   return int(budget / one) >= CAP ? CAP : int(budget / one);
 }
 
+// The decoupled epilogue (EPI = 2): each consumer group hands its FP64 row
+// sums to an update set of NU warps through a Y tile in shared memory
+// ([shot][2Np + 1], odd pitch) and goes on with its next item, so the DMMA
+// warps never wait on global memory; the update set runs the leap-frog
+// update with coalesced loads and stores of the contiguous state tile, the
+// sources, the energy terms and the receivers.
+template <int R, int NSG, int NG, int WM, int WN, int NU>
+struct D64WUpd {
+  typedef D64WCfg<R, NSG, NG, WM, WN> CF;
+  static constexpr int YP = R + 1;
+  static constexpr int YSZ = CF::ST * YP;  // doubles of one group's Y tile
+  static constexpr int NT = CF::NT + NG * NU * 32;
+  static constexpr size_t smem_bytes() {
+    return CF::smem_bytes() + (NU > 0 ? size_t(NG) * YSZ * sizeof(double) + size_t(2 * NG) * sizeof(uint64_t) : 0);
+  }
+};
+
+// Stages per group ring that fit beside the Y tiles (at most CAP).
+template <int R, int NG, int WM, int WN, int NU, int CAP>
+constexpr int d64w_fit_nsg_upd() {
+  constexpr size_t one = D64WUpd<R, 1, NG, WM, WN, NU>::smem_bytes();
+  constexpr size_t stage = size_t(NG) * (D64WCfg<R, 1, NG, WM, WN>::STAGE * sizeof(double) + 2 * sizeof(uint64_t));
+  constexpr size_t budget = 227 * 1024;
+  return int((budget - one) / stage) + 1 >= CAP ? CAP : int((budget - one) / stage) + 1;
+}
+
 // EPI selects where the epilogue gets u^k and u^{k-1}: 0 global loads issued
 // by the epilogue (fewest registers: the two consumer groups hide the
 // latency behind each other's products); 1 u^k from the diagonal block's
 // state stage and u^{k-1} requested before the products (no load latency in
 // the epilogue; 24 more registers per thread at 2Np = 42 with all rows per
-// warp, so it suits warp tiles of half the rows and a single group).
-template <int R, int NSG, int NG, int MINB = 1, int WM = 4, int WN = 2, int EPI = 0>
-__global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
+// warp, so it suits warp tiles of half the rows and a single group); 2 the
+// decoupled epilogue of NU update warps per group (D64WUpd).
+template <int R, int NSG, int NG, int MINB = 1, int WM = 4, int WN = 2, int EPI = 0, int NU = 0>
+__global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
     k_step_batched64w(const StepParams p, int* err_flag) {
   typedef D64WCfg<R, NSG, NG, WM, WN> CF;
+  typedef D64WUpd<R, NSG, NG, WM, WN, NU> UF;
+  static_assert((EPI == 2) == (NU > 0), "update warps exist exactly for the decoupled epilogue");
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
-  constexpr int NST = CF::NST;
+  constexpr int NST = CF::NST, YP = UF::YP, NTT = UF::NT;
+  constexpr int NCONS = NG * CF::NCW;    // DMMA warps
+  constexpr int PW = NCONS + NG * NU;    // the producer warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* stages = reinterpret_cast<double*>(smem_raw);
-  uint64_t* bfull = reinterpret_cast<uint64_t*>(stages + size_t(NST) * CF::STAGE);  // [NG][NSG] stage landed
-  uint64_t* bempty = bfull + NST;                                                    // [NG][NSG] stage consumed
-  volatile int* abort_s = reinterpret_cast<volatile int*>(bempty + NST);
+  double* ytiles = stages + size_t(NST) * CF::STAGE;                                    // [NG][ST][YP] (EPI = 2)
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(ytiles + (NU > 0 ? size_t(NG) * UF::YSZ : 0));  // [NG][NSG]
+  uint64_t* bempty = bfull + NST;                                                       // [NG][NSG] stage consumed
+  uint64_t* yfull = bempty + NST;                                                       // [NG] Y tile written (EPI = 2)
+  uint64_t* yempty = yfull + (NU > 0 ? NG : 0);                                         // [NG] Y tile consumed
+  volatile int* abort_s = reinterpret_cast<volatile int*>(yempty + (NU > 0 ? NG : 0));
 
   if (*reinterpret_cast<volatile int*>(err_flag) != 0) return;  // an earlier launch of the run timed out
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -107,9 +141,13 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
       fx_mbar_init(smem_u32(&bfull[i]), 1);
       fx_mbar_init(smem_u32(&bempty[i]), CF::NCW);
     }
+    for (int i = 0; i < (NU > 0 ? NG : 0); ++i) {
+      fx_mbar_init(smem_u32(&yfull[i]), CF::NCW);
+      fx_mbar_init(smem_u32(&yempty[i]), NU > 0 ? NU : 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = t; i < NST * CF::STAGE; i += CF::NT) stages[i] = 0.0;
+  for (int i = t; i < NST * CF::STAGE + (NU > 0 ? NG * UF::YSZ : 0); i += NTT) stages[i] = 0.0;
   __syncthreads();
 
   const int S = p.S;
@@ -118,7 +156,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
   const long long G = gridDim.x;
   const double* blocks = reinterpret_cast<const double*>(p.blocks);
 
-  if (warp == NG * CF::NCW) {
+  if (warp == PW) {
     // ---------------- producers: lane g fills ring g ----------------
     if (lane < NG) {
       const int g = lane;
@@ -160,7 +198,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
       }
       if (clock64() - t0 >= (1ll << 31)) *abort_s = 1;
     }
-  } else {
+  } else if (warp < NCONS) {
     // ---------------- consumers ----------------
     const int grp = warp / CF::NCW, wl = warp % CF::NCW, tl = t - grp * CF::NCW * 32;
     const int wm = wl % CF::WM, wn = wl / CF::WM;
@@ -178,6 +216,7 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
     const double* gst = stages + size_t(grp) * NSG * CF::STAGE;
     double en = 0.0;
     uint32_t j = 0;  // index into this group's ring
+    uint32_t m = 0;  // uses of this group's Y tile (EPI = 2)
     bool dead = false;
     long long it = 0;
     for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
@@ -249,6 +288,31 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
         __syncwarp();
         if (lane == 0) fx_mbar_arrive(smem_u32(&gempty[s]));
       }
+      if constexpr (EPI == 2) {
+        // ---- hand the row sums to the group's update set ----
+        if (!dead && m > 0) {
+          const bool okw = fx_wait(smem_u32(&yempty[grp]), (m - 1) & 1, abort_s);
+          if (__any_sync(0xffffffffu, !okw)) dead = true;
+        }
+        ++m;
+        if (dead) continue;
+        double* Y = ytiles + size_t(grp) * UF::YSZ;
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt) {
+          const int sl = (wm * MTW + mt) * 8 + gs;
+#pragma unroll
+          for (int q = 0; q < NTW; ++q) {
+            const int r0 = (nt0 + q) * 8 + 2 * tg;
+            if (q < ntn && r0 < R) {
+              Y[sl * YP + r0] = acc[mt][q][0];
+              Y[sl * YP + r0 + 1] = acc[mt][q][1];
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) fx_mbar_arrive(smem_u32(&yfull[grp]));
+        continue;
+      }
       // ---- epilogue (leap-frog, source, energy terms) ----
       if (!dead) {
         const double mi = p.minv[e];
@@ -318,6 +382,99 @@ __global__ void __launch_bounds__(D64WCfg<R, NSG, NG, WM, WN>::NT, MINB)
     if (p.energy != nullptr) {
       const double v = warp_sum(en);
       if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
+    }
+  } else {
+    if constexpr (EPI == 2) {
+      // ---------------- update sets: FP64 epilogue of the group's items ----------------
+      constexpr int NUT = (NU > 0 ? NU : 1) * 32;
+      const int ug = (warp - NCONS) / (NU > 0 ? NU : 1);
+      const int ut = t - (NCONS + ug * NU) * 32;  // thread within the set
+      const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
+      const double dt = p.dt;
+      const double* Y = ytiles + size_t(ug) * UF::YSZ;
+      constexpr int BATCH = 6;  // row pairs per thread and load batch
+      double en = 0.0;
+      uint32_t m = 0;
+      bool dead = false;
+      long long it = 0;
+      for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
+        if (int(it % NG) != ug) continue;
+        const int e = int(item / ntile), tile = int(item % ntile);
+        const int s0 = tile * ST, nsv = min(ST, S - s0);
+        const size_t base = (size_t(e) * S + s0) * R;  // the tile: nsv * R contiguous doubles
+        if (!dead) {
+          const bool okw = fx_wait(smem_u32(&yfull[ug]), m & 1, abort_s);
+          if (!__all_sync(0xffffffffu, okw)) dead = true;
+        }
+        ++m;
+        if (!dead) {
+          const double mi = p.minv[e];
+          const int npair = nsv * NP;
+          for (int pb = 0; pb < npair; pb += NUT * BATCH) {
+            // Row pair q = pb + NUT b + ut is entry 2q of the tile: shot
+            // q / NP, rows 2 (q % NP) and +1. Both levels' loads first.
+            double2 uu[BATCH], up[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; ++b) {
+              const int q = pb + NUT * b + ut;
+              const bool v = q < npair;
+              uu[b] = v ? __ldg(reinterpret_cast<const double2*>(p.x + base) + q) : make_double2(0.0, 0.0);
+              up[b] = (v && p.uprev) ? *(reinterpret_cast<const double2*>(p.uprev + base) + q) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; ++b) {
+              const int q = pb + NUT * b + ut;
+              if (q >= npair) continue;
+              const int sl = q / NP, r0 = 2 * (q - sl * NP);
+              const int sh = s0 + sl;
+              const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+              const double u[2] = {uu[b].x, uu[b].y}, upr[2] = {up[b].x, up[b].y};
+              double un[2];
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int r = r0 + h;
+                const int cmp = r / NP, ii = r - cmp * NP;
+                const double f =
+                    is_src ? p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
+                const double y = Y[sl * YP + r];
+                if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
+                else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
+                if (p.energy != nullptr) {
+                  const double d = un[h] - u[h];
+                  en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
+                }
+              }
+              *(reinterpret_cast<double2*>(p.out + base) + q) = make_double2(un[0], un[1]);
+              note_nonfinite(p, un[0], un[1]);
+            }
+          }
+        }
+        // u^{k+1} of the item is complete once the set passes this barrier
+        // (id 1 + group).
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + ug), "n"(NUT) : "memory");
+        if (!dead) {
+          if (p.rcv_ptr != nullptr) {
+            const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+            const long long slot = k % p.seis_cap;
+            for (int wk = ut; wk < (q1 - q0) * nsv * 2; wk += NUT) {
+              const int cmp = wk & 1, sl = (wk >> 1) % nsv, q = q0 + (wk >> 1) / nsv;
+              const int sh = s0 + sl;
+              const int rid = p.rcv_id[q];
+              const double* ph = p.rcv_phi + size_t(rid) * NP;
+              const double* un = p.out + base + size_t(sl) * R + cmp * NP;
+              double v = 0.0;
+              for (int ii = 0; ii < NP; ++ii) v += ph[ii] * un[ii];
+              p.seis[((size_t(sh) * p.seis_cap + slot) * p.nrcv + rid) * 2 + cmp] = v;
+            }
+          }
+          __syncwarp();
+          if (lane == 0) fx_mbar_arrive(smem_u32(&yempty[ug]));
+        }
+      }
+      if (p.energy != nullptr) {
+        const double v = warp_sum(en);
+        if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
+      }
     }
   }
   __syncthreads();
