@@ -71,7 +71,7 @@ def captured_traffic(kernel, ne, nshots):
 
 # Batched FP32 step kernels by variant (tsp_get_kernel_variant), for 2Np = 42.
 KERNELS = {0: "k_step_batched32k<42>", 1: "k_step_batched32p<42,64,4>", 2: "k_step_batched32<42>",
-           4: "k_step_batched_fx<42>", 7: "k_step_batched32w<42,3,3,2,1>", 8: "k_step_batched32w<42,3,3,2,0>"}
+           4: "k_step_batched_fx<42>", 7: "k_step_batched32w<42,3,3,2,1>", 8: "k_step_batched32w<42,3,3,2,2>"}
 
 
 def bytes_per_step(ne, Np, nnzb, nshots, precision):

@@ -340,7 +340,8 @@ int check_device_error(tsp_handle* h);
 // yet, so every output stays zero and nothing needs restoring -- timed with
 // CUDA events on the handle's stream; the fastest is kept. FP32 operator
 // (with its FP32 state shadow): 7 and 8 warp-specialised with bulk-copy rings
-// and 8 shots x several rows per lane (packed pair FMAs / scalar FMAs), 0 K
+// and 8 shots x several rows per lane (packed pair FMAs; 8 double-buffers the
+// operands), 0 K
 // split over warp groups, 1 pipelined
 // single group, 2 non-persistent, 4 tensor-core fixed point. FP64 operator: 5 and 6
 // warp-specialised DMMA (two consumer groups of 8 warps, or one group of 16
@@ -669,7 +670,8 @@ int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 // FP32-operator step on the CUDA cores with warp-specialised bulk-copy rings
-// (variants 7 and 8: packed pair FMAs / scalar FMAs): pairs of an FMA group
+// (variants 7 and 8: packed pair FMAs, the latter with the next K step's
+// operands fetched during the current step's FMAs): pairs of an FMA group
 // (NWG warps per item) and an update set of 2 warps (the FP64 epilogue), a
 // ring and a Y tile per pair; 6 FMA warps in all (3 pairs at 2Np = 42).
 template <int R, int F2>
@@ -720,7 +722,7 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) &&
       (h->kernel_variant == 7 || h->kernel_variant == 8)) {
-    if constexpr (R <= 56) return h->kernel_variant == 7 ? launch_s32w<R, 1>(h, p, st) : launch_s32w<R, 0>(h, p, st);
+    if constexpr (R <= 56) return h->kernel_variant == 7 ? launch_s32w<R, 1>(h, p, st) : launch_s32w<R, 2>(h, p, st);
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 42) {
