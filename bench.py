@@ -5,19 +5,23 @@
 Workload (default): the 64-shot batched configuration -- 200x100 jittered
 squares (40,000 triangles), Dubiner N=5 (1.68 M DOFs per shot), per-element
 log-normal vp, 64 Ricker shots at seeded interior points, 128 surface
-receivers, dt = 0.4 x CFL from a device power iteration -- in exact FP64
-(FP64 operator blocks and state, the products on the FP64 tensor cores;
---precision fp32 selects the FP32-operator form). One bench "step" is one
-leap-frog step of all 64 shots. Under torchrun each rank runs its own 64 shots (weak
+receivers, dt = 0.4 x CFL from a device power iteration -- in the mixed
+form: FP32 operator blocks, FP32 products and sums, FP64 state, recurrence,
+sources and receivers, the batched kernel chosen by the library's autotuner
+(its seismogram error against the reference's own FP64 run is reported;
+--precision fp64 selects exact FP64 on the FP64 tensor cores). One bench
+"step" is one leap-frog step of all 64 shots. Under torchrun each rank runs its own 64 shots (weak
 scaling, no collective in the data path); the timed region is bracketed by a
 barrier and a device synchronise, timed with CUDA events on the engine's
 stream, max over ranks.
 
 Also reported: the plain FP64 single-shot drop-in on the same mesh, the
-FP32-operator batched form, the seismogram error of each form against FP64
-from the CUDA-core FP64 kernel over the full step count,
-an end-to-end number through the public C-ABI with host buffers, the
-roofline of the step kernel and the reference's CPU path on a bounded sample.
+other batched form (exact FP64, or the FP32 operator), the seismogram error
+of each form against FP64 from the CUDA-core FP64 kernel over the full step
+count and against the reference's own run (a committed golden of 8 shots
+over 3,000 steps), the energy drift of each form, an end-to-end number
+through the public C-ABI with host buffers, the roofline of the step kernel
+and the reference's CPU path on a bounded sample.
 """
 from __future__ import annotations
 
@@ -71,7 +75,7 @@ def captured_traffic(kernel, ne, nshots):
 
 # Batched FP32 step kernels by variant (tsp_get_kernel_variant), for 2Np = 42.
 KERNELS = {0: "k_step_batched32k<42>", 1: "k_step_batched32p<42,64,4>", 2: "k_step_batched32<42>",
-           4: "k_step_batched_fx<42>", 7: "k_step_batched32w<42,3,3,2,1>", 8: "k_step_batched32w<42,3,3,2,2>"}
+           4: "k_step_batched_fx<42>", 7: "k_step_batched32w<42,3,3,2,1,6>", 8: "k_step_batched32w<42,4,2,2,1,3>"}
 
 
 def bytes_per_step(ne, Np, nnzb, nshots, precision):
@@ -187,12 +191,39 @@ def fp64_tensor_roofline(nnzb, Np, nshots, ms_step, kernel, device=0):
     flops = 2.0 * nnzb * (2 * Np) ** 2 * nshots
     ach = flops / (ms_step / 1e3) / 1e12
     meas = fp64_tensor_peak(device)
-    peak = meas if meas else FP64_TENSOR_NOMINAL_TFLOPS
-    src = ("measured on this GPU: register-only DMMA loop (tsp_fp64_tensor_peak)" if meas else
-           "nominal FP64 tensor rate (probe unavailable)")
+    peak = FP64_TENSOR_NOMINAL_TFLOPS
     return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-            "kernel": kernel, "peak_source": src, "peak_nominal": FP64_TENSOR_NOMINAL_TFLOPS,
-            "frac_of_nominal": ach / FP64_TENSOR_NOMINAL_TFLOPS, "algorithmic_flops_per_step": flops}
+            "kernel": kernel,
+            "peak_source": "nominal B200 FP64 tensor rate (no driver-measured FP64 figure exists)",
+            "peak_measured": meas, "frac_of_measured": (ach / meas) if meas else None,
+            "peak_measured_source": "register-only DMMA loop on this GPU (tsp_fp64_tensor_peak)",
+            "algorithmic_flops_per_step": flops}
+
+
+# FP32 CUDA-core peak of a B200: 148 SMs x 128 FP32 lanes x 2 flops x 1.965 GHz.
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def fp32_pipe_roofline(nnzb, Np, nshots, ms_step, kernel):
+    """The FP32-operator CUDA-core step against the FP32 pipe: algorithmic
+    flops 2 * nnzb * (2Np)^2 * shots per step."""
+    flops = 2.0 * nnzb * (2 * Np) ** 2 * nshots
+    ach = flops / (ms_step / 1e3) / 1e12
+    return {"bound": "fp32 pipe", "achieved": ach, "peak": FP32_SIMT_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+            "frac": ach / FP32_SIMT_NOMINAL_TFLOPS, "kernel": kernel,
+            "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 flops x 1.965 GHz",
+            "algorithmic_flops_per_step": flops}
+
+
+def graph_pieces(n, chunk=256):
+    """Graph replays tsp_run issues for n steps (pieces of `chunk` steps and
+    the powers of two of the remainder); each ends with one k_advance."""
+    pieces = 0
+    while n > 0:
+        ln = chunk if n >= chunk else 1 << (n.bit_length() - 1)
+        n -= ln
+        pieces += 1
+    return pieces
 
 
 def prepare(sim, prob, dt, nsteps):
@@ -469,7 +500,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
     ap.add_argument("--nshots", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--accuracy-steps", type=int, default=-1, help="steps of the FP64 comparison (-1: config's)")
@@ -537,7 +568,8 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": ("bf16x3 fixed-point operator, f64 state" if form == "fx" else
-                      "f32" if args.precision != "fp64" else "f64"), "data": "synthetic",
+                      "f32 operator (FP32 products and sums), f64 state" if args.precision == "fp32" else
+                      "bf16 operator, f64 state" if args.precision == "bf16" else "f64"), "data": "synthetic",
             "config": config_dict(args, prob), "dt": dt, "lmax": lmax,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": (captured_traffic(kernel, prob.mesh.ne, prob.nshots)
@@ -549,7 +581,7 @@ def main():
                          "kernel": kernel, "kernel_variant": variant,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_step": algo},
-            "gpu_launches": K + 1, "clocks": clocks}
+            "gpu_launches": K + graph_pieces(K), "clocks": clocks}
     if args.precision == "fp64" and prob.nshots > 1:
         # The FP64 batched step is bound by the FP64 tensor cores (DMMA), not HBM.
         line["roofline_hbm"] = line["roofline"]
@@ -559,6 +591,8 @@ def main():
         line["roofline"]["traffic"] = tr
         line["roofline"]["traffic_unit"] = "bytes per launch (ncu, profiles/traffic.json, scaled by element rows)"
         line["roofline_hbm"]["traffic"] = tr
+    if args.precision == "fp32" and prob.nshots > 1 and variant in (7, 8, 0, 1, 2):
+        line["roofline_fp32_pipe"] = fp32_pipe_roofline(sim.nnzb, prob.Np, prob.nshots, ms_step, kernel)
     sim.close()
 
     if rank == 0 and world == 1 and not args.no_extras:

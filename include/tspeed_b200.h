@@ -225,8 +225,7 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
 /* Kernel variant of the batched step chosen for this handle by the
  * autotuner at creation (or forced by TSP_BATCHED_VARIANT). FP32 operator:
  * 7 and 8 warp-specialised CUDA-core kernel with bulk-copy rings and
- * 8-shot register tiles (packed pair FMAs; 8 double-buffers the operands),
- * 0 K-split /
+ * 8-shot register tiles (6 or 8 FMA warps per SM), 0 K-split /
  * pipelined CUDA-core kernel, 1 pipelined CUDA-core kernel, 2 non-persistent
  * CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64
  * operator with several shots: 5 warp-specialised FP64 tensor-core (DMMA)

@@ -365,7 +365,7 @@ def test_fp32_ring_kernel(N, monkeypatch):
     and 8), 70 shots (one full and one partial 64-shot tile), with the energy
     monitor on: within the 1e-4 budget of the FP64 batched path shot by shot
     and as close to it as the k-split FP32 kernel (within 10x of its error);
-    the two product loops (7, 8) accumulate in the same order and agree to
+    the two configurations (7, 8) accumulate in the same order and agree to
     FP32 rounding."""
     m = W.jittered_rect(8, 5, 800.0, 500.0, seed=N + 190)
     rng = np.random.default_rng(N + 17)

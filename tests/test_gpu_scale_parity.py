@@ -137,7 +137,7 @@ def test_config3_sample_fp64_plain_row_kernel():
 @pytest.mark.parametrize("variant", [7, 8, 0, 4])
 def test_config3_sample_fp32_operator(variant, monkeypatch):
     """FP32 operator / FP64 state: the warp-specialised CUDA-core kernel
-    (7 packed pair FMAs, 8 scalar FMAs), the k-split CUDA-core kernel (0) and
+    (7: 6 FMA warps per SM, 8: 8 FMA warps), the k-split CUDA-core kernel (0) and
     the tensor-core fixed-point kernel (4), against the reference's FP64 run."""
     g = load_golden("g_config3_sample")
     seis, _ = run_golden(g, precision="fp32", monkeypatch=monkeypatch, variant=variant)

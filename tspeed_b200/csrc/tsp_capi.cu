@@ -340,8 +340,7 @@ int check_device_error(tsp_handle* h);
 // yet, so every output stays zero and nothing needs restoring -- timed with
 // CUDA events on the handle's stream; the fastest is kept. FP32 operator
 // (with its FP32 state shadow): 7 and 8 warp-specialised with bulk-copy rings
-// and 8 shots x several rows per lane (packed pair FMAs; 8 double-buffers the
-// operands), 0 K
+// and 8 shots x several rows per lane (6 or 8 FMA warps per SM), 0 K
 // split over warp groups, 1 pipelined
 // single group, 2 non-persistent, 4 tensor-core fixed point. FP64 operator: 5 and 6
 // warp-specialised DMMA (two consumer groups of 8 warps, or one group of 16
@@ -670,15 +669,17 @@ int launch_fx(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 }
 
 // FP32-operator step on the CUDA cores with warp-specialised bulk-copy rings
-// (variants 7 and 8: packed pair FMAs, the latter with the next K step's
-// operands fetched during the current step's FMAs): pairs of an FMA group
-// (NWG warps per item) and an update set of 2 warps (the FP64 epilogue), a
-// ring and a Y tile per pair; 6 FMA warps in all (3 pairs at 2Np = 42).
-template <int R, int F2>
+// and packed pair FMAs: pairs of an FMA group (NWG warps per item) and an
+// update set of 2 warps (the FP64 epilogue), a ring and a Y tile per pair.
+// V = 7: 6 FMA warps (3 pairs at 2Np = 42), 3-stage rings, 128 registers per
+// thread; V = 8: 8 FMA warps (4 pairs), 2-stage rings, 96 registers, smaller
+// update load batches.
+template <int R, int V>
 int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   constexpr int NWG = tsp::S32WCfg<R>::NWG;
-  constexpr int NGR = NWG == 1 ? 4 : 3;
-  constexpr int NU = 2;
+  // 2Np = 56: four pairs' rings no longer fit twice; variant 8 keeps three.
+  constexpr int NGR = V == 7 ? (NWG == 1 ? 4 : 3) : (NWG == 1 ? 6 : R <= 48 ? 4 : 3);
+  constexpr int NU = 2, UB = V == 7 ? 6 : 3;
   constexpr int NSG = tsp::s32w_fit_nsg<R, NGR, NU>();
   static_assert(NSG >= 2, "FP32 ring: two stages per pair must fit");
   typedef tsp::S32WLayout<R, NGR, NSG, NU> LY;
@@ -686,14 +687,14 @@ int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   static unsigned long long configured = 0;
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG, NU, F2>,
+    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched32w<R, NGR, NSG, NU, 1, UB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP32 ring kernel smem: ") + cudaGetErrorString(e));
     configured |= bit;
   }
   const long long items = (long long)h->ne * ((h->S + 63) / 64);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
-  tsp::k_step_batched32w<R, NGR, NSG, NU, F2><<<grid, LY::NT, smem, st>>>(p, h->d_err);
+  tsp::k_step_batched32w<R, NGR, NSG, NU, 1, UB><<<grid, LY::NT, smem, st>>>(p, h->d_err);
   return TSP_OK;
 }
 
@@ -722,7 +723,7 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) &&
       (h->kernel_variant == 7 || h->kernel_variant == 8)) {
-    if constexpr (R <= 56) return h->kernel_variant == 7 ? launch_s32w<R, 1>(h, p, st) : launch_s32w<R, 2>(h, p, st);
+    if constexpr (R <= 56) return h->kernel_variant == 7 ? launch_s32w<R, 7>(h, p, st) : launch_s32w<R, 8>(h, p, st);
   }
   if (h->shadow && (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst) && h->kernel_variant != 2) {
     if constexpr (R <= 42) {

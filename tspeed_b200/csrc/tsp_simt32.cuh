@@ -110,10 +110,9 @@ __device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, fl
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
 
-// F2 selects the product loop: scalar FMAs (0), packed pair FMAs (1), or
-// packed pair FMAs with the next step's operands fetched during the current
-// step's FMAs (2).
-template <int R, int NGR, int NSG, int NU, int F2>
+// F2 selects packed pair FMAs (1) or scalar FMAs (0) for the products.
+// UB: row pairs per update thread and load batch.
+template <int R, int NGR, int NSG, int NU, int F2, int UB = 6>
 __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
     k_step_batched32w(const StepParams p, int* err_flag) {
   typedef S32WCfg<R> CF;
@@ -229,41 +228,6 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
         }
         const float* Bs = gst + size_t(s) * CF::STAGE + rbase;
         const float* Xs = gst + size_t(s) * CF::STAGE + CF::BSZ + 4 * sg;
-        if constexpr (F2 == 2) {
-          // Two operand sets in turn (R is even): step kk + 1's operands are
-          // loaded and splatted while step kk's FMAs issue, with no copies
-          // between the sets.
-          unsigned long long xa[4], ba[RL], xb[4], bb[RL];
-          auto fetch = [&](int kk, unsigned long long* x4, unsigned long long* bs) {
-            const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(Xs + kk * ST);
-            const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(Xs + kk * ST + 32);
-            x4[0] = v0.x;
-            x4[1] = v0.y;
-            x4[2] = v1.x;
-            x4[3] = v1.y;
-#pragma unroll
-            for (int i = 0; i < RL; i += 2) {
-              const float2 b2 = *reinterpret_cast<const float2*>(Bs + kk * KP + i);
-              bs[i] = f32x2_splat(b2.x);
-              bs[i + 1] = f32x2_splat(b2.y);
-            }
-          };
-          auto fma_step = [&](const unsigned long long* x4, const unsigned long long* bs) {
-#pragma unroll
-            for (int i = 0; i < RL; ++i)
-#pragma unroll
-              for (int mm = 0; mm < 4; ++mm) acc2[i][mm] = ffma2(x4[mm], bs[i], acc2[i][mm]);
-          };
-          static_assert(R % 2 == 0, "2Np is even");
-          fetch(0, xa, ba);
-#pragma unroll 1
-          for (int kk = 0; kk < R; kk += 2) {
-            fetch(kk + 1, xb, bb);
-            fma_step(xa, ba);
-            if (kk + 2 < R) fetch(kk + 2, xa, ba);
-            fma_step(xb, bb);
-          }
-        } else {
 #pragma unroll 2
         for (int kk = 0; kk < R; ++kk) {
           float bv[RL];
@@ -293,11 +257,10 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
               for (int q = 0; q < 8; ++q) acc[i][q] = fmaf(xv[q], bv[i], acc[i][q]);
           }
         }
-        }
         __syncwarp();
         if (lane == 0) fx_mbar_arrive(smem_u32(&gempty[s]));
       }
-      if constexpr (F2 != 0) {
+      if constexpr (F2) {
 #pragma unroll
         for (int i = 0; i < RL; ++i)
 #pragma unroll
@@ -327,7 +290,7 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
     const long long k = (p.step_base ? *p.step_base : 0) + p.rel;
     const double dt = p.dt;
     float* Y = ybuf + size_t(ug) * LY::YSZ;
-    constexpr int BATCH = 6;  // row pairs per thread and load batch
+    constexpr int BATCH = UB;  // row pairs per thread and load batch
     double en = 0.0;
     uint32_t m = 0;
     bool dead = false;
