@@ -351,6 +351,13 @@ int check_device_error(tsp_handle* h);
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, int, int, int>, int> g_tune_cache;
 
+// The autotuner's earlier choice for a handle of this shape, or -1.
+int tune_cached(const tsp_handle* h) {
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  auto it = g_tune_cache.find(std::make_tuple(h->device, h->prec, h->R, h->S, h->ne));
+  return it == g_tune_cache.end() ? -1 : it->second;
+}
+
 int autotune(tsp_handle* h) {
   NvtxRange nvtx_("autotune");
   const bool fx_ok = h->fx;
@@ -470,8 +477,10 @@ int finish_create(tsp_handle* h) {
   }
   // The tensor-core kernel's slice buffers exist when it is forced or is a
   // candidate of the autotuner.
+  // (Not when the autotuner already chose another kernel for this shape.)
   const bool fx_ok = h->shadow && h->op_kind == TSP_OP_EXPLICIT && h->R <= 56;
-  h->fx = fx_ok && (h->kernel_variant == 4 || h->kernel_variant < 0);
+  const int cached = h->kernel_variant < 0 ? tune_cached(h) : -1;
+  h->fx = fx_ok && (h->kernel_variant == 4 || (h->kernel_variant < 0 && (cached < 0 || cached == 4)));
   if (h->fx && (rc = fx_dispatch(h, true, 0))) return rc;
   if ((rc = dalloc(h, &h->d_step, 1))) return rc;
   TSP_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
