@@ -46,3 +46,38 @@ def l2_proj_tol(g):
     xy = g["xy"]
     area = float(np.ptp(xy[:, 0]) * np.ptp(xy[:, 1]))
     return 1e-13 * np.sqrt(area) * 1.0 + 1e-12 * float(g["l2_proj"])
+
+
+# ---- operator storage formats, emulated on the oracle's FP64 blocks ----
+
+def bf16_round(x):
+    """float32 values rounded to bfloat16 (round to nearest, ties to even),
+    returned as float64."""
+    x = np.asarray(x, np.float32)
+    b = x.view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def pow2_scale(m):
+    """Power-of-two scale 2^ceil(log2 m) (1 for m = 0): values / scale lie in [-1, 1]."""
+    m = np.asarray(m, np.float64)
+    return np.where(m > 0, 2.0 ** np.ceil(np.log2(np.where(m > 0, m, 1.0))), 1.0)
+
+
+def bf16_block_scaled(blocks):
+    """The library's BF16 storage: per block, scale = 2^ceil(log2 max|float(B)|),
+    entries bf16(float(B) / scale) (the device's k_assemble)."""
+    b32 = np.asarray(blocks).astype(np.float32)
+    sc = pow2_scale(np.abs(b32).max(axis=(1, 2)))[:, None, None]
+    return bf16_round(b32 / sc) * sc
+
+
+def fixed_point_rows(blocks, planes):
+    """Fixed point with a shared power-of-two exponent per block row and
+    8 bits per BF16 plane after a 9-bit leading plane (the tensor-core form's
+    slicing with `planes` planes): 8 * planes + 1 significant bits."""
+    B = np.asarray(blocks, np.float64)
+    m = np.abs(B).max(axis=2, keepdims=True)
+    ex = np.ceil(np.log2(np.where(m > 0, m, 1.0)))
+    return np.rint(B * 2.0 ** (8 * planes - ex)) * 2.0 ** (ex - 8 * planes)

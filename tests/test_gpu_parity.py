@@ -193,24 +193,47 @@ def test_batched_partial_shot_tiles_match_oracle(N):
         assert rel(seis[k], s_ref) < 1e-12
 
 
-# FP32 blocks meet the 1e-4 seismogram budget. Plain BF16 blocks do not:
-# B u cancels heavily (penalty and stiffness terms of a smooth field), so the
-# error grows with the storage rounding unit (2^-9 vs 2^-24); the bound below
-# only checks that the BF16 form runs and stays bounded.
-@pytest.mark.parametrize("precision,tol", [("fp32", 1e-4), ("bf16", 1.0)])
-def test_mixed_precision_close_to_fp64(precision, tol):
+# FP32 blocks meet the 1e-4 seismogram budget. BF16 blocks with per-block
+# scales do not: B u cancels heavily (penalty and stiffness terms of a smooth
+# field), so the error grows with the storage rounding unit (2^-9 vs 2^-24;
+# tests/test_precision_study.py). The BF16 path is therefore checked for what
+# it computes: the leap-frog of the BF16-stored operator, emulated on the
+# oracle's blocks (the device's FP32 products and sums add errors of the FP32
+# form's size, far below the BF16 storage error).
+def test_fp32_operator_close_to_fp64():
     g = __import__("conftest").load_golden("g_config1_small")
     with sim_from_golden(g, "fp64") as s:
         s.first_step()
         s.run(int(g["nsteps"]) - 1)
         ref = s.seismograms(0, int(g["nsteps"]))[0]
-    with sim_from_golden(g, precision) as s:
+    with sim_from_golden(g, "fp32") as s:
         s.first_step()
         s.run(int(g["nsteps"]) - 1)
         lo = s.seismograms(0, int(g["nsteps"]))[0]
     err = rel(lo, ref)
-    print(precision, "seismogram rel L2 error vs fp64:", err)
-    assert err < tol
+    print("fp32 seismogram rel L2 error vs fp64:", err)
+    assert err < 1e-4
+
+
+def test_bf16_operator_matches_its_storage_emulation():
+    from helpers import bf16_block_scaled
+    g = __import__("conftest").load_golden("g_config1_small")
+    n = int(g["nsteps"])
+    with sim_from_golden(g, "bf16") as s:
+        s.first_step()
+        s.run(n - 1)
+        lo = s.seismograms(0, n)[0]
+    o = oracle_setup(g)
+    N = int(g["N"])
+    Np = (N + 1) * (N + 2) // 2
+    run = lambda blocks: O.leapfrog(o["row_ptr"], o["cols"], blocks, o["minv"], len(g["tri"]), Np,  # noqa: E731
+                                    float(g["dt"]), n, o["src_elem"], o["src_phi"], o["F"], o["rcv_elem"],
+                                    o["rcv_phi"])[1]
+    emul = run(bf16_block_scaled(o["blocks"]))
+    ref = run(o["blocks"])
+    e_emul, e_fp64 = rel(lo, emul), rel(lo, ref)
+    print("bf16: vs its storage emulation", e_emul, "vs fp64", e_fp64)
+    assert e_emul < 1e-3 and e_fp64 > 0.1
 
 
 def test_fp32_batched_shadow_kernel_close_to_fp64_and_resumable():
