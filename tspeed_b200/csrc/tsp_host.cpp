@@ -1,6 +1,7 @@
 // Host-side setup for the tspeed_b200 engine (see tsp_host.h).
 #include "tsp_host.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -346,31 +347,51 @@ Geometry make_geometry(int32_t ne, const double* xy, const int32_t* tri) {
 
 bool build_neighbours(int32_t ne, const int32_t* tri, int32_t* neigh, int32_t* nedge, std::string* err) {
   // Directed edge (a -> b) of face l; a neighbour owns the reversed edge.
+  // The directed edges are bucketed by their first vertex (a CSR over the
+  // vertices, a handful of edges per vertex), so finding the reversed edge
+  // (b -> a) scans bucket b: O(ne) in all, no hashing.
   static const int ends[3][2] = {{1, 2}, {2, 0}, {0, 1}};
-  std::unordered_map<uint64_t, int64_t> table;
-  table.reserve(size_t(ne) * 3 * 2);
-  auto key = [](uint32_t a, uint32_t b) { return (uint64_t(a) << 32) | b; };
+  int32_t nv = 0;
+  for (size_t i = 0; i < size_t(ne) * 3; ++i) nv = std::max(nv, tri[i] + 1);
+  std::vector<int32_t> start(size_t(nv) + 1, 0);
+  for (size_t i = 0; i < size_t(ne) * 3; ++i) {
+    const size_t e = i / 3;
+    const int l = int(i % 3);
+    start[size_t(tri[3 * e + ends[l][0]]) + 1]++;
+  }
+  for (int32_t v = 0; v < nv; ++v) start[size_t(v) + 1] += start[v];
+  std::vector<int32_t> fill(start.begin(), start.end() - 1);
+  std::vector<int32_t> to(size_t(ne) * 3), owner(size_t(ne) * 3);  // bucket entries: end vertex, element*3 + face
   for (int32_t e = 0; e < ne; ++e)
     for (int l = 0; l < 3; ++l) {
-      const uint32_t a = uint32_t(tri[3 * size_t(e) + ends[l][0]]), b = uint32_t(tri[3 * size_t(e) + ends[l][1]]);
-      auto ins = table.emplace(key(a, b), int64_t(e) * 3 + l);
-      if (!ins.second) {
-        if (err) {
-          std::ostringstream os;
-          os << "directed edge (" << a << "," << b << ") shared by elements " << ins.first->second / 3 << " and " << e
-             << " (clockwise or overlapping triangles)";
-          *err = os.str();
+      const int32_t a = tri[3 * size_t(e) + ends[l][0]], b = tri[3 * size_t(e) + ends[l][1]];
+      // The same directed edge twice: clockwise or overlapping triangles.
+      for (int32_t q = start[a]; q < fill[a]; ++q)
+        if (to[q] == b) {
+          if (err) {
+            std::ostringstream os;
+            os << "directed edge (" << a << "," << b << ") shared by elements " << owner[q] / 3 << " and " << e
+               << " (clockwise or overlapping triangles)";
+            *err = os.str();
+          }
+          return false;
         }
-        return false;
-      }
+      to[fill[a]] = b;
+      owner[fill[a]] = 3 * e + l;
+      ++fill[a];
     }
   for (int32_t e = 0; e < ne; ++e)
     for (int l = 0; l < 3; ++l) {
-      const uint32_t a = uint32_t(tri[3 * size_t(e) + ends[l][0]]), b = uint32_t(tri[3 * size_t(e) + ends[l][1]]);
-      auto it = table.find(key(b, a));
-      if (it != table.end() && it->second / 3 != e) {
-        neigh[3 * size_t(e) + l] = int32_t(it->second / 3);
-        nedge[3 * size_t(e) + l] = int32_t(it->second % 3);
+      const int32_t a = tri[3 * size_t(e) + ends[l][0]], b = tri[3 * size_t(e) + ends[l][1]];
+      int32_t found = -1;
+      for (int32_t q = start[b]; q < start[size_t(b) + 1]; ++q)
+        if (to[q] == a) {
+          found = owner[q];
+          break;
+        }
+      if (found >= 0 && found / 3 != e) {
+        neigh[3 * size_t(e) + l] = found / 3;
+        nedge[3 * size_t(e) + l] = found % 3;
       } else {
         neigh[3 * size_t(e) + l] = -1;
         nedge[3 * size_t(e) + l] = -1;
@@ -457,51 +478,54 @@ void locate_points(int N, int32_t ne, const double* xy, const int32_t* tri, cons
       elem[k] = locate_point(N, ne, xy, tri, g, pts[2 * k], pts[2 * k + 1], phi + size_t(k) * Np, basis);
     return;
   }
-  // Uniform grid over the padded boxes, about one element per cell; each
-  // cell lists, in increasing id, every element whose padded box meets it.
-  std::vector<double> boxes(size_t(ne) * 4);
+  // One pass over the elements in increasing id; the points (few against
+  // the elements) are bucketed in a uniform grid, and each element tests
+  // the points in the cells its padded box meets. A point takes the first
+  // element that contains it: the same lowest-id element as a scan.
   double X0 = 1e300, X1 = -1e300, Y0 = 1e300, Y1 = -1e300;
-  for (int32_t e = 0; e < ne; ++e) {
-    double* b = &boxes[size_t(e) * 4];
-    element_box(xy, tri, e, b);
-    X0 = std::fmin(X0, b[0]);
-    X1 = std::fmax(X1, b[1]);
-    Y0 = std::fmin(Y0, b[2]);
-    Y1 = std::fmax(Y1, b[3]);
-  }
-  const double W = std::fmax(X1 - X0, 1e-300), H = std::fmax(Y1 - Y0, 1e-300);
-  const double cells = std::fmax(1.0, double(ne));
-  int nx = int(std::ceil(std::sqrt(cells * W / H)));
-  int ny = int(std::ceil(cells / nx));
-  nx = std::max(1, std::min(nx, 1 << 14));
-  ny = std::max(1, std::min(ny, 1 << 14));
-  auto cx = [&](double x) { return std::min(nx - 1, std::max(0, int((x - X0) / W * nx))); };
-  auto cy = [&](double y) { return std::min(ny - 1, std::max(0, int((y - Y0) / H * ny))); };
-  const size_t ncell = size_t(nx) * ny;
-  std::vector<int64_t> start(ncell + 1, 0);
-  for (int32_t e = 0; e < ne; ++e) {
-    const double* b = &boxes[size_t(e) * 4];
-    for (int iy = cy(b[2]); iy <= cy(b[3]); ++iy)
-      for (int ix = cx(b[0]); ix <= cx(b[1]); ++ix) start[size_t(iy) * nx + ix + 1]++;
-  }
-  for (size_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
-  std::vector<int32_t> list(size_t(start[ncell]));
-  std::vector<int64_t> fill(start.begin(), start.end() - 1);
-  for (int32_t e = 0; e < ne; ++e) {
-    const double* b = &boxes[size_t(e) * 4];
-    for (int iy = cy(b[2]); iy <= cy(b[3]); ++iy)
-      for (int ix = cx(b[0]); ix <= cx(b[1]); ++ix) list[size_t(fill[size_t(iy) * nx + ix]++)] = e;
-  }
+  int32_t left = 0;
   for (int32_t k = 0; k < npts; ++k) {
-    const double px = pts[2 * k], py = pts[2 * k + 1];
     elem[k] = -1;
-    if (!(px >= X0 && px <= X1 && py >= Y0 && py <= Y1)) continue;  // outside every padded box (or NaN)
-    const size_t c = size_t(cy(py)) * nx + cx(px);
-    for (int64_t i = start[c]; i < start[c + 1]; ++i)
-      if (try_element(N, basis, xy, tri, g, list[size_t(i)], px, py, phi + size_t(k) * Np)) {
-        elem[k] = list[size_t(i)];
-        break;
-      }
+    const double px = pts[2 * k], py = pts[2 * k + 1];
+    if (!(std::isfinite(px) && std::isfinite(py))) continue;
+    X0 = std::fmin(X0, px);
+    X1 = std::fmax(X1, px);
+    Y0 = std::fmin(Y0, py);
+    Y1 = std::fmax(Y1, py);
+    ++left;
+  }
+  if (left == 0) return;
+  const int G = std::max(1, std::min(1024, int(std::ceil(std::sqrt(double(left))))));
+  const double W = std::fmax(X1 - X0, 1e-300), H = std::fmax(Y1 - Y0, 1e-300);
+  auto cx = [&](double x) { return std::min(G - 1, std::max(0, int((x - X0) / W * G))); };
+  auto cy = [&](double y) { return std::min(G - 1, std::max(0, int((y - Y0) / H * G))); };
+  std::vector<int32_t> start(size_t(G) * G + 1, 0);
+  std::vector<int32_t> list(static_cast<size_t>(left));
+  for (int32_t k = 0; k < npts; ++k)
+    if (std::isfinite(pts[2 * k]) && std::isfinite(pts[2 * k + 1]))
+      start[size_t(cy(pts[2 * k + 1])) * G + cx(pts[2 * k]) + 1]++;
+  for (size_t c = 0; c < size_t(G) * G; ++c) start[c + 1] += start[c];
+  {
+    std::vector<int32_t> fill(start.begin(), start.end() - 1);
+    for (int32_t k = 0; k < npts; ++k)
+      if (std::isfinite(pts[2 * k]) && std::isfinite(pts[2 * k + 1]))
+        list[size_t(fill[size_t(cy(pts[2 * k + 1])) * G + cx(pts[2 * k])]++)] = k;
+  }
+  for (int32_t e = 0; e < ne && left > 0; ++e) {
+    double b[4];
+    element_box(xy, tri, e, b);
+    if (b[1] < X0 || b[0] > X1 || b[3] < Y0 || b[2] > Y1) continue;  // meets no point
+    for (int iy = cy(b[2]); iy <= cy(b[3]); ++iy)
+      for (int ix = cx(b[0]); ix <= cx(b[1]); ++ix)
+        for (int32_t i = start[size_t(iy) * G + ix]; i < start[size_t(iy) * G + ix + 1]; ++i) {
+          const int32_t k = list[size_t(i)];
+          const double px = pts[2 * k], py = pts[2 * k + 1];
+          if (elem[k] >= 0 || px < b[0] || px > b[1] || py < b[2] || py > b[3]) continue;
+          if (try_element(N, basis, xy, tri, g, e, px, py, phi + size_t(k) * Np)) {
+            elem[k] = e;
+            --left;
+          }
+        }
   }
 }
 
