@@ -1219,7 +1219,7 @@ int tsp_create(const tsp_problem* P, tsp_handle** out) {
     }
   }
   // Large meshes exceed the 2^31-1 grid limit only beyond 2 G blocks.
-  tsp::k_assemble<<<unsigned(h->nnzb), 256, 0, h->stream>>>(ap);
+  tsp::k_assemble<<<unsigned(h->ne), 256, 0, h->stream>>>(ap);
   {
     cudaError_t ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);

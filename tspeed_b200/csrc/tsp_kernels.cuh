@@ -1866,25 +1866,17 @@ __device__ __forceinline__ double block_entry(const AssembleParams& p, int e, in
   return v;
 }
 
-// One CTA per block.
+// One CTA per element row: the row's set-up (the elastic tensor in the
+// element's frame, the face terms of its three faces and of the neighbours'
+// matching faces) is shared by the row's blocks and computed by seven
+// threads at once; then the row's blocks are written entry by entry.
 __global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
-  const int b = blockIdx.x;
-  __shared__ int s_e;
-  __shared__ double alpha[16], betas[24], cmn[12], betan[8];
+  const int e = blockIdx.x;
+  __shared__ double alpha[16], betas[24], cmn[12], betan[4][8];
   __shared__ float s_max[8];
-  // Find the row of block b (binary search over row_ptr).
-  if (threadIdx.x == 0) {
-    int lo = 0, hi = p.ne - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (p.row_ptr[mid] <= b) lo = mid;
-      else hi = mid - 1;
-    }
-    s_e = lo;
-  }
-  __syncthreads();
-  const int e = s_e, c = p.col[b], face = p.bface[b];
-  if (threadIdx.x == 0) {
+  const int rb = p.row_ptr[e], nb = min(4, p.row_ptr[e + 1] - rb);
+  const int t = threadIdx.x;
+  if (t == 0) {
     const double lam = p.lam[e], mu = p.mu[e];
     const double* iJ = p.invJ + 4 * size_t(e);
     // C^{mn}_{kl} (k,l index physical derivatives), row-major [mn][k*2+l].
@@ -1892,58 +1884,65 @@ __global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
     for (int mn = 0; mn < 4; ++mn)
       for (int a = 0; a < 2; ++a)
         for (int bb = 0; bb < 2; ++bb) {
-          double s = 0.0;
+          double sum = 0.0;
           for (int kk = 0; kk < 2; ++kk)
-            for (int ll = 0; ll < 2; ++ll) s += C[mn][kk * 2 + ll] * iJ[a + 2 * kk] * iJ[bb + 2 * ll];
-          alpha[mn * 4 + a * 2 + bb] = s;
+            for (int ll = 0; ll < 2; ++ll) sum += C[mn][kk * 2 + ll] * iJ[a + 2 * kk] * iJ[bb + 2 * ll];
+          alpha[mn * 4 + a * 2 + bb] = sum;
         }
-    for (int l = 0; l < 3; ++l) {
-      const int nb = p.neigh[3 * size_t(e) + l];
-      if (nb < 0) {
-        for (int q = 0; q < 8; ++q) betas[l * 8 + q] = 0.0;
-        for (int q = 0; q < 4; ++q) cmn[l * 4 + q] = 0.0;
-        continue;
-      }
+  } else if (t <= 3) {
+    const int l = t - 1;
+    const int nbr = p.neigh[3 * size_t(e) + l];
+    if (nbr < 0) {
+      for (int q = 0; q < 8; ++q) betas[l * 8 + q] = 0.0;
+      for (int q = 0; q < 4; ++q) cmn[l * 4 + q] = 0.0;
+    } else {
       face_beta(p, e, l, betas + l * 8);
-      const double al = harm(p.lam[e], p.lam[nb]), am = harm(p.mu[e], p.mu[nb]);
+      const double al = harm(p.lam[e], p.lam[nbr]), am = harm(p.mu[e], p.mu[nbr]);
       const double n0 = p.enrm[6 * size_t(e) + 2 * l], n1 = p.enrm[6 * size_t(e) + 2 * l + 1];
       cmn[l * 4 + 0] = (al + 2 * am) * n0 * n0 + 2 * am * n1 * n1;
       cmn[l * 4 + 3] = (al + 2 * am) * n1 * n1 + 2 * am * n0 * n0;
       cmn[l * 4 + 1] = al * n0 * n1;
       cmn[l * 4 + 2] = al * n0 * n1;
     }
-    if (face >= 0) face_beta(p, c, p.nedge[3 * size_t(e) + face], betan);
+  } else if (t <= 7 && t - 4 < nb) {
+    const int q = t - 4, face = p.bface[rb + q];
+    if (face >= 0) face_beta(p, p.col[rb + q], p.nedge[3 * size_t(e) + face], betan[q]);
   }
   __syncthreads();
   const int R = 2 * p.Np;
   const int RR = R * R;
-  float amax = 0.0f;
-  if (p.prec == 2) {
-    for (int t = threadIdx.x; t < RR; t += blockDim.x) {
-      const int cc = t / R, r = t - cc * R;
-      amax = fmaxf(amax, float(fabs(block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan))));
+  for (int q = 0; q < nb; ++q) {
+    const int b = rb + q, c = p.col[b], face = p.bface[b];
+    float inv_sc = 1.0f;
+    if (p.prec == 2) {
+      float amax = 0.0f;
+      for (int i = t; i < RR; i += blockDim.x) {
+        const int cc = i / R, r = i - cc * R;
+        amax = fmaxf(amax, float(fabs(block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan[q]))));
+      }
+      for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      if ((t & 31) == 0) s_max[t >> 5] = amax;
+      __syncthreads();
+      if (t == 0) {
+        float m = 0.0f;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
+        // Power-of-two scale: values land in [-1, 1] and scaling is exact.
+        const float sc = (m > 0.0f) ? exp2f(ceilf(log2f(m))) : 1.0f;
+        s_max[0] = sc;
+        p.scale[b] = sc;
+      }
+      __syncthreads();
+      inv_sc = 1.0f / s_max[0];
+      __syncthreads();  // s_max is reused by the next block
     }
-    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = amax;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      float m = 0.0f;
-      for (int w = 0; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, s_max[w]);
-      // Power-of-two scale: values land in [-1, 1] and scaling is exact.
-      const float sc = (m > 0.0f) ? exp2f(ceilf(log2f(m))) : 1.0f;
-      s_max[0] = sc;
-      p.scale[b] = sc;
+    for (int i = t; i < RR; i += blockDim.x) {
+      const int cc = i / R, r = i - cc * R;  // column-major storage: (r, cc) at cc*pitch + r
+      const double v = block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan[q]);
+      const size_t o = size_t(b) * R * p.pitch + size_t(cc) * p.pitch + r;
+      if (p.prec == 0) reinterpret_cast<double*>(p.out)[o] = v;
+      else if (p.prec == 1) reinterpret_cast<float*>(p.out)[o] = float(v);
+      else reinterpret_cast<__nv_bfloat16*>(p.out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
     }
-    __syncthreads();
-  }
-  const float inv_sc = (p.prec == 2) ? 1.0f / s_max[0] : 1.0f;
-  for (int t = threadIdx.x; t < RR; t += blockDim.x) {
-    const int cc = t / R, r = t - cc * R;  // column-major storage: (r, cc) at cc*pitch + r
-    const double v = block_entry(p, e, c, face, r, cc, alpha, betas, cmn, betan);
-    const size_t o = size_t(b) * R * p.pitch + size_t(cc) * p.pitch + r;
-    if (p.prec == 0) reinterpret_cast<double*>(p.out)[o] = v;
-    else if (p.prec == 1) reinterpret_cast<float*>(p.out)[o] = float(v);
-    else reinterpret_cast<__nv_bfloat16*>(p.out)[o] = __float2bfloat16_rn(float(v) * inv_sc);
   }
 }
 
