@@ -693,6 +693,7 @@ int launch_s32w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
   static_assert(NSG >= 2, "FP32 ring: two stages per pair must fit");
   typedef tsp::S32WLayout<R, NGR, NSG, NU> LY;
   const size_t smem = LY::smem_bytes();
+  static_assert(LY::smem_bytes() <= 227 * 1024, "FP32 ring kernel shared memory");
   static unsigned long long configured = 0;
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {

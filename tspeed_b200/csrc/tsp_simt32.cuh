@@ -83,14 +83,20 @@ struct S32WLayout {
   }
 };
 
-// Stages per pair ring that fit in shared memory beside the Y tiles.
+// Stages per pair ring (at most 6) that fit in shared memory beside the Y
+// tiles; 0 if not even one does.
 template <int R, int NGR, int NU>
 constexpr int s32w_fit_nsg() {
-  typedef S32WLayout<R, NGR, 1, NU> L1;
-  constexpr size_t fixed = L1::smem_bytes() - size_t(NGR) * S32WCfg<R>::STAGE * sizeof(float);
-  constexpr size_t per = size_t(NGR) * (S32WCfg<R>::STAGE * sizeof(float) + 2 * sizeof(uint64_t));
   constexpr size_t budget = 227 * 1024;
-  return int((budget - fixed) / per) >= 6 ? 6 : int((budget - fixed) / per);
+  int n = 6;
+  while (n > 0) {
+    const size_t bytes = size_t(NGR) * n * S32WCfg<R>::STAGE * sizeof(float) +
+                         size_t(NGR) * S32WLayout<R, NGR, 1, NU>::YSZ * sizeof(float) +
+                         size_t(2 * NGR * n + 2 * NGR) * sizeof(uint64_t) + 16;
+    if (bytes <= budget) break;
+    --n;
+  }
+  return n;
 }
 
 // Packed FP32 FMA on pairs (Blackwell fma.rn.f32x2; one instruction per two
@@ -108,6 +114,88 @@ __device__ __forceinline__ unsigned long long f32x2_splat(float v) {
 }
 __device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, float& hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+// Shots of a 64-shot tile whose source lies in element e (bit sl), for steps
+// that still have a force sample; the same in every lane of the warp.
+__device__ __forceinline__ unsigned long long tile_source_mask(const StepParams& p, int e, int s0, int nsv,
+                                                               long long k, int ln) {
+  if (k >= p.nF) return 0ull;
+  const bool a = ln < nsv && p.src_elem[s0 + ln] == e;
+  const bool b = ln + 32 < nsv && p.src_elem[s0 + 32 + ln] == e;
+  return (unsigned long long)__ballot_sync(0xffffffffu, a) | ((unsigned long long)__ballot_sync(0xffffffffu, b) << 32);
+}
+
+// FP64 epilogue of one item's state tile by an update set of NUT threads, UB
+// row pairs per thread and load batch (both levels' loads of a batch first).
+// Reads the FP32 row sums from the Y tile ([shot][R + 1]) and writes u^{k+1}
+// back into it in FP32 for the shadow. (A software-pipelined form, the next
+// batch's loads issued before the current batch is stored, needs twice the
+// load registers and spilled at the 96 registers per thread of these
+// kernels: slower.)
+template <int R, int NUT, int UB>
+__device__ __forceinline__ void s32_update_tile(const StepParams& p, float* Y, int e, int s0, int nsv, size_t base,
+                                                int ut, long long k, double dt, double& en) {
+  constexpr int NP = R / 2, YP = R + 1, STEP = NUT * UB;
+  static_assert(S32WCfg<R>::ST == 64, "one 64-bit source mask per shot tile");
+  const double mi = p.minv[e];
+  const int npair = nsv * NP;
+  const double2* xs = reinterpret_cast<const double2*>(p.x + base);
+  const double2* ps = p.uprev ? reinterpret_cast<const double2*>(p.uprev + base) : nullptr;
+  // The update warps are few and run dependent chains, so the epilogue keeps
+  // per-pair work to the FP64 recurrence: the shots whose source lies in this
+  // element are found once per tile (bit sl of smask, two loads per lane),
+  // and a non-finite u^{k+1} is caught by one FMA per value (inf * 0 and
+  // NaN * 0 are NaN) and reported once per tile.
+  const unsigned long long smask = tile_source_mask(p, e, s0, nsv, k, ut & 31);
+  double chk = 0.0;
+  // Row pair q = pb + NUT b + ut is entry 2q of the tile: shot q / NP, rows
+  // 2 (q % NP) and +1 (coalesced loads and stores).
+  for (int q0 = 0; q0 < npair; q0 += STEP) {
+    double2 uu[UB], up[UB];
+#pragma unroll
+    for (int b = 0; b < UB; ++b) {
+      const int q = q0 + NUT * b + ut;
+      const bool v = q < npair;
+      uu[b] = v ? __ldg(xs + q) : make_double2(0.0, 0.0);
+      up[b] = (v && ps) ? ps[q] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int b = 0; b < UB; ++b) {
+      const int q = q0 + NUT * b + ut;
+      if (q >= npair) continue;
+      const int sl = q / NP, r0 = 2 * (q - sl * NP);
+      const double u[2] = {uu[b].x, uu[b].y}, upr[2] = {up[b].x, up[b].y};
+      double yv[2] = {double(Y[sl * YP + r0]), double(Y[sl * YP + r0 + 1])};
+      if (smask != 0 && ((smask >> sl) & 1)) {
+        const int sh = s0 + sl;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + h, cmp = r / NP, ii = r - cmp * NP;
+          yv[h] -= p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii];
+        }
+      }
+      double un[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * yv[h]);
+        else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * yv[h]);  // kModeFirst, uprev = v0
+        chk = __fma_rn(un[h], 0.0, chk);
+      }
+      if (p.energy != nullptr) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double d = un[h] - u[h];
+          // y of the energy term is the product B u^k without the source.
+          en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * double(Y[sl * YP + r0 + h]);
+        }
+      }
+      Y[sl * YP + r0] = float(un[0]);
+      Y[sl * YP + r0 + 1] = float(un[1]);
+      *(reinterpret_cast<double2*>(p.out + base) + q) = make_double2(un[0], un[1]);
+    }
+  }
+  if (chk != chk && p.nonfinite != nullptr) *p.nonfinite = 1;
 }
 
 // F2 selects packed pair FMAs (1) or scalar FMAs (0) for the products.
@@ -309,57 +397,21 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
         if (!__all_sync(0xffffffffu, okw)) dead = true;
       }
       ++m;
-      if (!dead) {
-        const double mi = p.minv[e];
-        const int npair = nsv * NP;
-        for (int pb = 0; pb < npair; pb += NUT * BATCH) {
-          // Row pair q = pb + NUT b + ut is entry 2q of the tile: shot q / NP,
-          // rows 2 (q % NP) and +1. Both levels' loads first (coalesced).
-          double2 uu[BATCH], up[BATCH];
-#pragma unroll
-          for (int b = 0; b < BATCH; ++b) {
-            const int q = pb + NUT * b + ut;
-            const bool v = q < npair;
-            uu[b] = v ? __ldg(reinterpret_cast<const double2*>(p.x + base) + q) : make_double2(0.0, 0.0);
-            up[b] = (v && p.uprev) ? *(reinterpret_cast<const double2*>(p.uprev + base) + q) : make_double2(0.0, 0.0);
-          }
-#pragma unroll
-          for (int b = 0; b < BATCH; ++b) {
-            const int q = pb + NUT * b + ut;
-            if (q >= npair) continue;
-            const int sl = q / NP, r0 = 2 * (q - sl * NP);
-            const int sh = s0 + sl;
-            const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
-            const double u[2] = {uu[b].x, uu[b].y}, upr[2] = {up[b].x, up[b].y};
-            double un[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int r = r0 + h;
-              const int cmp = r / NP, ii = r - cmp * NP;
-              const double f = is_src ? p.F[(size_t(sh) * p.nF + k) * 2 + cmp] * p.src_phi[size_t(sh) * NP + ii] : 0.0;
-              const double y = double(Y[sl * YP + r]);
-              if (p.mode == kModeStep) un[h] = (2 * u[h] - upr[h]) + mi * ((-dt * dt) * (y - f));
-              else un[h] = (u[h] + dt * upr[h]) - mi * (dt * dt / 2 * (y - f));  // kModeFirst, uprev = v0
-              if (p.energy != nullptr) {
-                const double d = un[h] - u[h];
-                en += 0.5 * (d * d) / (mi * dt * dt) + 0.5 * un[h] * y;
-              }
-              Y[sl * YP + r] = float(un[h]);
-            }
-            *(reinterpret_cast<double2*>(p.out + base) + q) = make_double2(un[0], un[1]);
-            note_nonfinite(p, un[0], un[1]);
-          }
-        }
-      }
+      if (!dead) s32_update_tile<R, NUT, BATCH>(p, Y, e, s0, nsv, base, ut, k, dt, en);
       // u^{k+1} of the item (FP64 in global memory, FP32 in the Y tile) is
       // complete once the whole set passes this barrier (id 1 + pair).
       asm volatile("bar.sync %0, %1;" ::"r"(1 + ug), "n"(NUT) : "memory");
       if (!dead) {
         // FP32 shadow of u^{k+1}, transposed: rows of 64 shots (shots beyond
-        // S stay zero), 32 consecutive floats per warp store.
-        for (int idx = ut; idx < R * ST; idx += NUT) {
-          const int r = idx / ST, sl = idx - r * ST;
-          p.x32_out[(tix * R + r) * ST + sl] = sl < nsv ? Y[sl * YP + r] : 0.0f;
+        // S stay zero), four shots per 16-byte store.
+        for (int i4 = ut; i4 < R * (ST / 4); i4 += NUT) {
+          const int r = i4 / (ST / 4), sl = (i4 - r * (ST / 4)) * 4;
+          float4 v;
+          v.x = sl < nsv ? Y[sl * YP + r] : 0.0f;
+          v.y = sl + 1 < nsv ? Y[(sl + 1) * YP + r] : 0.0f;
+          v.z = sl + 2 < nsv ? Y[(sl + 2) * YP + r] : 0.0f;
+          v.w = sl + 3 < nsv ? Y[(sl + 3) * YP + r] : 0.0f;
+          *reinterpret_cast<float4*>(p.x32_out + (tix * R + r) * ST + sl) = v;
         }
         // Receivers of this element.
         if (p.rcv_ptr != nullptr) {
