@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
     uint64_t* gempty = bempty + grp * NSG;
     const double* gst = stages + size_t(grp) * NSG * CF::STAGE;
     double en = 0.0;
+    double chk = 0.0;  // NaN once a non-finite u^{k+1} was written (inf * 0 and NaN * 0 are NaN)
     uint32_t j = 0;  // index into this group's ring
     uint32_t m = 0;  // uses of this group's Y tile (EPI = 2)
     bool dead = false;
@@ -351,7 +352,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
               }
             }
             *reinterpret_cast<double2*>(p.out + me + r0) = make_double2(un[0], un[1]);
-            note_nonfinite(p, un[0], un[1]);
+            chk = __fma_rn(un[0], 0.0, __fma_rn(un[1], 0.0, chk));
           }
         }
       }
@@ -379,6 +380,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
         }
       }
     }
+    if (chk != chk && p.nonfinite != nullptr) *p.nonfinite = 1;
     if (p.energy != nullptr) {
       const double v = warp_sum(en);
       if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
@@ -394,6 +396,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
       const double* Y = ytiles + size_t(ug) * UF::YSZ;
       constexpr int BATCH = 6;  // row pairs per thread and load batch
       double en = 0.0;
+      double chk = 0.0;
       uint32_t m = 0;
       bool dead = false;
       long long it = 0;
@@ -445,7 +448,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
                 }
               }
               *(reinterpret_cast<double2*>(p.out + base) + q) = make_double2(un[0], un[1]);
-              note_nonfinite(p, un[0], un[1]);
+              chk = __fma_rn(un[0], 0.0, __fma_rn(un[1], 0.0, chk));
             }
           }
         }
@@ -471,6 +474,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
           if (lane == 0) fx_mbar_arrive(smem_u32(&yempty[ug]));
         }
       }
+      if (chk != chk && p.nonfinite != nullptr) *p.nonfinite = 1;
       if (p.energy != nullptr) {
         const double v = warp_sum(en);
         if (lane == 0 && v != 0.0) atomicAdd(p.energy + (k % p.energy_cap), v);
