@@ -160,10 +160,12 @@ def estimate_dt(sim, cfl_fraction=0.4, iters=60):
 # 5 warp-specialised DMMA, two consumer groups of 8 warps with a 3-stage ring
 # each; 6 the same kernel with one group of 16 warps and a 6-stage ring; 9 and
 # 10 the same kernel with the epilogue in update warps (two groups, 2-stage
-# rings / one group, 5-stage ring); 3 the single-role DMMA kernel; 2 the
-# CUDA-core kernel.
-D64_KERNELS = {5: "k_step_batched64w<42,3,2,1,8,1,0,0>", 6: "k_step_batched64w<42,6,1,1,8,2,1,0>",
-               9: "k_step_batched64w<42,2,2,1,8,1,2,1>", 10: "k_step_batched64w<42,5,1,1,8,2,2,2>",
+# rings / one group, 5-stage ring); 13 as 5 with u^{k-1} requested before
+# the products under a warpgroup register split; 3 the single-role DMMA
+# kernel; 2 the CUDA-core kernel.
+D64_KERNELS = {5: "k_step_batched64w<42,3,2,1,8,1,0,0,0>", 6: "k_step_batched64w<42,6,1,1,8,2,1,0,0>",
+               9: "k_step_batched64w<42,2,2,1,8,1,2,1,0>", 10: "k_step_batched64w<42,5,1,1,8,2,2,2,0>",
+               13: "k_step_batched64w<42,3,2,1,8,1,3,0,112>",
                3: "k_step_batched64d<42>", 2: "k_step_batched<42,double>"}
 
 # Nominal dense FP64 tensor-core rate of a B200 (DMMA); MEASURED_PEAKS.json

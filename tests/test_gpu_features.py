@@ -160,14 +160,14 @@ def test_fp64_autotuner_choice_and_override(monkeypatch):
     rcv = W.surface_receivers(m, 4)
     n = 40
     out = {}
-    for forced in (None, "5", "6", "9", "10", "3", "2"):
+    for forced in (None, "5", "13", "6", "9", "10", "3", "2"):
         if forced is None:
             monkeypatch.delenv("TSP_BATCHED_VARIANT", raising=False)
         else:
             monkeypatch.setenv("TSP_BATCHED_VARIANT", forced)
         with capi.Simulation.create(m.xy, m.tri, 4, lam, mu, rho, shots, rcv, penalty=10.0) as s:
             v = s.kernel_variant
-            assert v in (5, 6, 9, 10, 3, 2) if forced is None else v == int(forced)
+            assert v in (5, 13, 6, 9, 10, 3, 2) if forced is None else v == int(forced)
             s.set_dt(2e-4)
             for k in range(len(shots)):
                 s.set_ricker(k, 25.0, 0.04, -1.0, 1, n)

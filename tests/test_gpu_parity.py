@@ -664,7 +664,9 @@ def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
     warp-specialised persistent kernel in its two configurations
     (TSP_BATCHED_VARIANT=5: two consumer groups with a ring each; =6: one
     group of 16 warps whose epilogue takes u^k from shared memory; =9 and
-    =10: the DMMA warps hand their row sums to update warps) and the
+    =10: the DMMA warps hand their row sums to update warps; =13: as 5 with
+    u^{k-1} requested before the products, under a warpgroup register split)
+    and the
     single-role one (=3); the register-staged CUDA-core kernel (=2) computes
     the same products in another order: all agree to rounding, over full and
     partial shot tiles, with the energy monitor on. Without the variable the
@@ -678,7 +680,7 @@ def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
     n = 80
     out = {}
     dt = None
-    for variant in ("auto", "5", "6", "9", "10", "3", "2"):
+    for variant in ("auto", "5", "13", "6", "9", "10", "3", "2"):
         if variant != "auto":
             monkeypatch.setenv("TSP_BATCHED_VARIANT", variant)
         else:
@@ -695,10 +697,10 @@ def test_fp64_batched_tensor_core_matches_cuda_core(N, monkeypatch):
             s.run(n - 1)
             out[variant] = (s.seismograms(0, n), s.u_all(), s.energy(1, n - 1))
             if variant == "auto":
-                assert s.kernel_variant in (5, 6, 9, 10, 3, 2)
+                assert s.kernel_variant in (5, 13, 6, 9, 10, 3, 2)
             else:
                 assert s.kernel_variant == int(variant)
-    for v in ("auto", "5", "6", "9", "10", "3"):
+    for v in ("auto", "5", "13", "6", "9", "10", "3"):
         for i in range(3):
             print("N", N, v, i, rel(out[v][i], out["2"][i]))
             assert rel(out[v][i], out["2"][i]) < 1e-13

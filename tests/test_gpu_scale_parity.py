@@ -77,7 +77,7 @@ def test_config1_full_fp64_single_shot(op):
     assert e_s < FP64_TOL and e_u < FP64_TOL
 
 
-@pytest.mark.parametrize("variant", [5, 6, 9, 10, 3, 2])
+@pytest.mark.parametrize("variant", [5, 13, 6, 9, 10, 3, 2])
 def test_config1_full_fp64_batched(variant, monkeypatch):
     """The batched FP64 kernels need several shots: the golden's source twice."""
     g = load_golden("g_config1_full")
@@ -100,7 +100,7 @@ def test_config1_full_fp32_operator(shots, variant, monkeypatch):
 
 # ---- the 64-shot configuration's shape on its x0.2 sample (8 shots) ----
 
-@pytest.mark.parametrize("variant", [5, 6, 9, 10, 3, 2])
+@pytest.mark.parametrize("variant", [5, 13, 6, 9, 10, 3, 2])
 def test_config3_sample_fp64_batched(variant, monkeypatch):
     g = load_golden("g_config3_sample")
     seis, us = run_golden(g, monkeypatch=monkeypatch, variant=variant)

@@ -365,7 +365,7 @@ int autotune(tsp_handle* h) {
   if (fp64_batched) {
     if (h->kernel_variant >= 0) {
       const int v = h->kernel_variant;
-      if (v != 2 && v != 3 && v != 6 && v != 9 && v != 10) h->kernel_variant = 5;
+      if (v != 2 && v != 3 && v != 6 && v != 9 && v != 10 && v != 13) h->kernel_variant = 5;
       return TSP_OK;
     }
   } else if (h->kernel_variant >= 0 || !h->shadow) {
@@ -380,7 +380,7 @@ int autotune(tsp_handle* h) {
     if (it != g_tune_cache.end()) cached = it->second;
   }
   std::vector<int> cands;
-  if (fp64_batched) cands = {5, 9, 10, 6, 3, 2};
+  if (fp64_batched) cands = {5, 13, 9, 10, 6, 3, 2};
   else if (h->R <= 42) cands = {7, 8, 0, 1, 2};
   else if (h->R <= 56) cands = {7, 8, 0, 2};
   else cands = {2};
@@ -550,27 +550,49 @@ int launch_d64(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
 // before the products, so it has no latency to hide.
 template <int R, int V>
 int launch_d64w(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
-  constexpr int NG = (V == 5 && R <= 56) ? 2 : 1;
+  constexpr bool two = V == 5 || V == 13;
+  constexpr int NG = (two && R <= 56) ? 2 : 1;
   constexpr int ST = tsp::D64WCfg<R, 1, NG>::ST;
-  constexpr int NCW = (V == 5) ? 8 : 16;
+  constexpr int NCW = two ? 8 : 16;
   constexpr int WM = ST / 8, WN = NCW / WM;
-  constexpr int EPI = (V == 5) ? 0 : 1;
+  constexpr int EPI = (V == 5) ? 0 : (V == 13) ? 3 : 1;
+  // V = 13: variant 5's tiles, u^{k-1} requested before the products and u^k
+  // loaded by the epilogue (EPI = 3); the 24 registers that takes come from a
+  // warpgroup register split (two consumer groups only; else as 5).
+  constexpr int RA = (V == 13 && NG == 2) ? 112 : 0;
   constexpr int NSG = tsp::d64w_fit_nsg<R, NG, WM, WN, (NG == 1 ? 6 : 4)>();
   static_assert(NSG >= 2, "FP64 DMMA ring: two stages per group must fit");
   typedef tsp::D64WCfg<R, NSG, NG, WM, WN> CF;
+  constexpr int NT = tsp::d64w_nt<R, NSG, NG, WM, WN, 0, RA>();
   const size_t smem = CF::smem_bytes();
   static unsigned long long configured = 0;  // one bit per device
+  static unsigned long long split_ok = 0;    // one bit per device: the register split fits the launch
   const unsigned long long bit = 1ull << (h->device & 63);
   if (!(configured & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    auto kern = tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI, 0, RA>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return fail(h, TSP_ERR_CUDA, std::string("FP64 batched kernel smem: ") + cudaGetErrorString(e));
+    if constexpr (RA > 0) {
+      // setmaxnreg.inc waits until the CTA's pool (threads x registers at
+      // launch) has the registers: launch only if the split fits.
+      cudaFuncAttributes fa;
+      if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess)
+        return fail(h, TSP_ERR_CUDA, "FP64 batched kernel attributes");
+      const long long pool = (long long)fa.numRegs * NT;
+      const long long need = (long long)CF::NCW * NG * 32 * RA + (long long)(NT - CF::NCW * NG * 32) * tsp::kD64ProducerRegs;
+      if (pool >= need && fa.numRegs <= RA) split_ok |= bit;
+    }
     configured |= bit;
+  }
+  if constexpr (RA > 0) {
+    if (!(split_ok & bit)) return launch_d64w<R, 5>(h, p, st);  // the same product and results
+  } else if constexpr (V == 13) {
+    return launch_d64w<R, 5>(h, p, st);  // one consumer group: no split, variant 5's form
   }
   // Persistent: one CTA per SM.
   const long long items = (long long)h->ne * ((h->S + CF::ST - 1) / CF::ST);
   const unsigned grid = unsigned(std::min<long long>(items, h->num_sms));
-  tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI><<<grid, CF::NT, smem, st>>>(p, h->d_err);
+  tsp::k_step_batched64w<R, NSG, NG, 1, WM, WN, EPI, 0, RA><<<grid, NT, smem, st>>>(p, h->d_err);
   return TSP_OK;
 }
 
@@ -766,6 +788,7 @@ int launch_R(tsp_handle* h, const tsp::StepParams& p, cudaStream_t st) {
       (p.mode == tsp::kModeStep || p.mode == tsp::kModeFirst))
     return h->kernel_variant == 3    ? launch_d64<R>(h, p, st)
            : h->kernel_variant == 6  ? launch_d64w<R, 6>(h, p, st)
+           : h->kernel_variant == 13 ? launch_d64w<R, 13>(h, p, st)
            : h->kernel_variant == 9  ? launch_d64u<R, 9>(h, p, st)
            : h->kernel_variant == 10 ? launch_d64u<R, 10>(h, p, st)
                                      : launch_d64w<R, 5>(h, p, st);

@@ -107,21 +107,41 @@ constexpr int d64w_fit_nsg_upd() {
   return int((budget - one) / stage) + 1 >= CAP ? CAP : int((budget - one) / stage) + 1;
 }
 
+// Threads of the kernel: with a register split (RA > 0) the producer warp is
+// padded to a whole warpgroup, so that every warpgroup is all consumers or
+// the producer's.
+template <int R, int NSG, int NG, int WM, int WN, int NU, int RA>
+constexpr int d64w_nt() {
+  constexpr int nt = D64WUpd<R, NSG, NG, WM, WN, NU>::NT;
+  return RA > 0 ? ((nt / 32 + 3) / 4) * 128 : nt;
+}
+// Registers per thread of the producer warpgroup under a register split.
+constexpr int kD64ProducerRegs = 24;
+
 // EPI selects where the epilogue gets u^k and u^{k-1}: 0 global loads issued
 // by the epilogue (fewest registers: the two consumer groups hide the
 // latency behind each other's products); 1 u^k from the diagonal block's
 // state stage and u^{k-1} requested before the products (no load latency in
 // the epilogue; 24 more registers per thread at 2Np = 42 with all rows per
 // warp, so it suits warp tiles of half the rows and a single group); 2 the
-// decoupled epilogue of NU update warps per group (D64WUpd).
-template <int R, int NSG, int NG, int MINB = 1, int WM = 4, int WN = 2, int EPI = 0, int NU = 0>
-__global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
+// decoupled epilogue of NU update warps per group (D64WUpd); 3 u^{k-1} requested
+// before the products as in 1 and u^k loaded by the epilogue (an L2 hit: the
+// diagonal block's state copy brought the element's tile there), half the
+// extra registers of 1.
+// RA > 0: register split -- the consumer warpgroups raise their registers to
+// RA per thread (setmaxnreg), the producer warpgroup lowers its own to
+// kD64ProducerRegs; the launch must hold at least NCONS * 32 * RA +
+// (threads - NCONS * 32) * kD64ProducerRegs registers (the host checks the
+// compiled register count before launching), so that the raise never waits.
+// It gives EPI = 1 (latency-free epilogue) room with two consumer groups.
+template <int R, int NSG, int NG, int MINB = 1, int WM = 4, int WN = 2, int EPI = 0, int NU = 0, int RA = 0>
+__global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
     k_step_batched64w(const StepParams p, int* err_flag) {
   typedef D64WCfg<R, NSG, NG, WM, WN> CF;
   typedef D64WUpd<R, NSG, NG, WM, WN, NU> UF;
   static_assert((EPI == 2) == (NU > 0), "update warps exist exactly for the decoupled epilogue");
   constexpr int NP = R / 2, KP = CF::KP, ST = CF::ST, NTL = CF::NTL, MTW = CF::MTW, NTW = CF::NTW;
-  constexpr int NST = CF::NST, YP = UF::YP, NTT = UF::NT;
+  constexpr int NST = CF::NST, YP = UF::YP, NTT = d64w_nt<R, NSG, NG, WM, WN, NU, RA>();
   constexpr int NCONS = NG * CF::NCW;    // DMMA warps
   constexpr int PW = NCONS + NG * NU;    // the producer warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -155,6 +175,11 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
   const long long nitems = (long long)p.ne * ntile;
   const long long G = gridDim.x;
   const double* blocks = reinterpret_cast<const double*>(p.blocks);
+  if constexpr (RA > 0) {
+    static_assert(NU == 0 && NCONS % 4 == 0 && RA % 8 == 0 && RA <= 256, "register split: consumer warpgroups");
+    if (warp < NCONS) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(RA));
+    else asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kD64ProducerRegs));
+  }
 
   if (warp == PW) {
     // ---------------- producers: lane g fills ring g ----------------
@@ -225,6 +250,16 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
       const int e = int(item / ntile), tile = int(item % ntile);
       const int s0 = tile * ST;
       const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      // The epilogue's scalar inputs, requested now so that they arrive during
+      // the products: the element's inverse-mass factor and, per m-tile,
+      // whether the shot's source lies in this element.
+      const double mi_e = p.minv[e];
+      int src_e[MTW];
+#pragma unroll
+      for (int mt = 0; mt < MTW; ++mt) {
+        const int sh = s0 + (wm * MTW + mt) * 8 + gs;
+        src_e[mt] = (sh < S) ? p.src_elem[sh] : -1;
+      }
       // u^{k-1} of this warp's outputs, requested now and used by the
       // epilogue: the loads overlap the products. u^k comes from the
       // diagonal block's state stage (the element's own tile) when the row
@@ -243,7 +278,7 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
           uk[mt][q] = make_double2(0.0, 0.0);
         }
       }
-      const bool diag_first = EPI != 0 && p.col[rb] == e;
+      const bool diag_first = EPI == 1 && p.col[rb] == e;
       double acc[MTW][NTW][2];
 #pragma unroll
       for (int mt = 0; mt < MTW; ++mt)
@@ -316,13 +351,13 @@ __global__ void __launch_bounds__(D64WUpd<R, NSG, NG, WM, WN, NU>::NT, MINB)
       }
       // ---- epilogue (leap-frog, source, energy terms) ----
       if (!dead) {
-        const double mi = p.minv[e];
+        const double mi = mi_e;
 #pragma unroll
         for (int mt = 0; mt < MTW; ++mt) {
           const int sh = s0 + (wm * MTW + mt) * 8 + gs;
           if (sh >= S) continue;
           const size_t me = (size_t(e) * S + sh) * R;
-          const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+          const bool is_src = (src_e[mt] == e) && (k < p.nF);
           double Fk[2] = {0.0, 0.0};
           if (is_src) {
             Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
