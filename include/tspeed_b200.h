@@ -230,9 +230,11 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
  * CUDA-core kernel, 4 tensor-core fixed-point kernel. FP64
  * operator with several shots: 5 warp-specialised FP64 tensor-core (DMMA)
  * kernel with two consumer groups of 8 warps (8 shots x all rows per warp),
- * 6 the same kernel with one group of 16 warps (8 shots x half the rows) and
- * an epilogue without load latency, 3 single-role DMMA kernel, 2 CUDA-core
- * kernel.
+ * 13 the same tiles with u^{k-1} requested before the products (a
+ * warpgroup register split gives the registers), 6 the same kernel with one
+ * group of 16 warps (8 shots x half the rows) and an epilogue without load
+ * latency, 9 and 10 the epilogue in update warps, 3 single-role DMMA kernel,
+ * 2 CUDA-core kernel.
  * No counterpart in the reference (its step is a single CPU path). */
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant);
 
