@@ -381,6 +381,9 @@ def reference_arm(args):
     nsteps = max(10, args.steps)
     v, sample = cpu_reference_sample(nprocs=ncores, nsteps=nsteps, scale=args.ref_scale)
     cfg = config_dict(args, None)
+    # What this arm actually ran (a bounded sample of the configuration, per
+    # DOF-step), so that its config does not read as the full configuration.
+    cfg["reference_sample"] = sample
     if v is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
