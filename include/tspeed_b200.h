@@ -50,7 +50,8 @@ typedef enum {
   TSP_ERR_MESH = -6,        /* malformed mesh (clockwise triangle, non-manifold edge, bad file) */
   TSP_ERR_NONFINITE = -7,   /* NaN/Inf detected in the state */
   TSP_ERR_TIMEOUT = -8,     /* a bounded device-side wait gave up */
-  TSP_ERR_UNSUPPORTED = -9  /* option not built for this degree/precision */
+  TSP_ERR_UNSUPPORTED = -9, /* option not built for this degree/precision */
+  TSP_ERR_INDEX = -10       /* checked build: a kernel read a gather index out of range */
 } tsp_status;
 
 /* Storage of the operator blocks. The state, the recurrence, M^-1 and the
@@ -237,6 +238,18 @@ int tsp_run_timed(tsp_handle* h, int64_t nsteps, double* ms);
  * 2 CUDA-core kernel.
  * No counterpart in the reference (its step is a single CPU path). */
 int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant);
+
+/* 1 if this library is the checked build (libtspeed_b200_checked.so,
+ * compiled with TSP_CHECKED), else 0. In the checked build every gather
+ * index the step kernels read -- row extents of the block pattern,
+ * neighbour ids, source elements, receiver ranges and ids, mesh neighbours
+ * of the matrix-free kernel -- is range-checked on the device; an index out
+ * of range is replaced by a valid one (no out-of-bounds access) and
+ * recorded, and the next read-back or timed run (tsp_run_timed, tsp_get_u,
+ * tsp_get_u_all, tsp_get_seismograms, tsp_field_values, tsp_write_field,
+ * tsp_l2_error) returns TSP_ERR_INDEX naming the index kind and value. Results are then void. No counterpart
+ * in the reference (it has no device code; its host checks call exit()). */
+int tsp_checked_build(void);
 
 /* Number of leap-frog steps done (first_step counts as 1) and the
  * reference's M_last_time. */

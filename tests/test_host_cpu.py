@@ -32,6 +32,21 @@ def test_library_exports_every_declared_symbol():
     assert set(capi.SIGNATURES) == syms
 
 
+def test_checked_build_exports_the_same_symbols():
+    """The TSP_CHECKED library (device-side index checks) exports every
+    declared entry point and reports itself as checked; the default library
+    does not."""
+    import ctypes
+    path = os.path.join(ROOT, "tspeed_b200", "libtspeed_b200_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("checked library not built (python -m tspeed_b200.build --checked)")
+    L = ctypes.CDLL(path)
+    missing = [s for s in header_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    assert L.tsp_checked_build() == 1
+    assert capi.lib().tsp_checked_build() == (1 if os.environ.get("TSP_CHECKED") == "1" else 0)
+
+
 def test_version_string():
     assert b"sm_100a" in capi.lib().tsp_version()
 

@@ -13,7 +13,10 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libtspeed_b200.so")
+# TSP_CHECKED=1 selects the build whose kernels range-check every gather
+# index on the device (tsp_checked_build; TSP_ERR_INDEX on a failure).
+LIB_PATH = os.path.join(_HERE, "libtspeed_b200_checked.so" if os.environ.get("TSP_CHECKED") == "1"
+                        else "libtspeed_b200.so")
 
 TSP_PREC = {"fp64": 0, "fp32": 1, "bf16": 2}
 TSP_OP = {"explicit": 0, "matrix_free": 1}
@@ -21,7 +24,7 @@ TSP_OP = {"explicit": 0, "matrix_free": 1}
 TSP_BASIS = {"dubiner": 0, "ba": 1, "boundary_adapted": 1}
 STATUS = {0: "TSP_OK", -1: "TSP_ERR_ARG", -2: "TSP_ERR_CUDA", -3: "TSP_ERR_NOMEM", -4: "TSP_ERR_STATE",
           -5: "TSP_ERR_NOT_FOUND", -6: "TSP_ERR_MESH", -7: "TSP_ERR_NONFINITE", -8: "TSP_ERR_TIMEOUT",
-          -9: "TSP_ERR_UNSUPPORTED"}
+          -9: "TSP_ERR_UNSUPPORTED", -10: "TSP_ERR_INDEX"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -61,6 +64,7 @@ SIGNATURES = {
     "tsp_run_timed": (C.c_int, [C.c_void_p, C.c_int64, _dp]),
     "tsp_get_progress": (C.c_int, [C.c_void_p, _lp, _dp]),
     "tsp_get_kernel_variant": (C.c_int, [C.c_void_p, _ip]),
+    "tsp_checked_build": (C.c_int, []),
     "tsp_get_u": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
     "tsp_get_u_all": (C.c_int, [C.c_void_p, _dp]),
     "tsp_get_seismograms": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _dp]),

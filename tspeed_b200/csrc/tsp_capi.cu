@@ -855,6 +855,7 @@ int launch_step(tsp_handle* h, int mode, const double* x, const double* uprev, d
   p.seis_cap = h->seis_cap;
   p.energy = (sample && h->energy_on) ? h->d_energy : nullptr;
   p.nonfinite = sample ? h->d_err + 1 : nullptr;
+  p.nnzb = h->nnzb;
   p.energy_cap = h->energy_cap;
   p.acc = h->d_acc;
   p.x32_in = nullptr;
@@ -947,6 +948,26 @@ void dev_to_ref(const tsp_handle* h, int shot, const double* src_all, double* ds
 
 // Reports a bounded device-side wait that gave up (after a synchronisation).
 int check_device_error(tsp_handle* h) {
+#ifdef TSP_CHECKED
+  // Checked build: the first gather index a kernel found out of range since
+  // the last check (site, value); the kernels clamped it, the results are void.
+  {
+    unsigned long long w = 0;
+    TSP_CUDA(h, cudaMemcpyFromSymbolAsync(&w, tsp::g_index_check, sizeof(w), 0, cudaMemcpyDeviceToHost, h->stream));
+    TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (w != 0) {
+      const unsigned long long zero = 0;
+      TSP_CUDA(h, cudaMemcpyToSymbolAsync(tsp::g_index_check, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
+      TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+      static const char* const kSites[] = {"?", "row extent of element", "neighbour id", "source element",
+                                           "receiver range", "receiver id", "mesh neighbour"};
+      const unsigned site = unsigned(w >> 32);
+      return fail(h, TSP_ERR_INDEX,
+                  std::string("device index check: ") + kSites[site < 7 ? site : 0] + " out of range (value " +
+                      std::to_string(int(unsigned(w & 0xffffffffu))) + "); results invalid");
+    }
+  }
+#endif
   if (!h->d_err) return TSP_OK;
   int v = 0;
   TSP_CUDA(h, copy_sync(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1625,6 +1646,14 @@ int tsp_get_kernel_variant(const tsp_handle* h, int32_t* variant) {
   return TSP_OK;
 }
 
+int tsp_checked_build(void) {
+#ifdef TSP_CHECKED
+  return 1;
+#else
+  return 0;
+#endif
+}
+
 int tsp_get_progress(const tsp_handle* h, int64_t* steps_done, double* last_time) {
   if (!h) return TSP_ERR_ARG;
   if (steps_done) *steps_done = h->steps_done;
@@ -1698,7 +1727,11 @@ int tsp_get_seismograms(tsp_handle* h, int64_t k0, int64_t nk, double* out) {
       k += run;
     }
   TSP_CUDA(h, cudaStreamSynchronize(h->stream));
+#ifdef TSP_CHECKED
+  return check_device_error(h);  // the samples are void after an index failure
+#else
   return TSP_OK;
+#endif
 }
 
 int tsp_enable_energy(tsp_handle* h, int32_t on) {
@@ -2327,6 +2360,7 @@ extern "C" int tsp_estimate_lmax_noalloc(tsp_handle* h, int32_t iters, double* l
   p.bscale = (h->prec == TSP_PREC_BF16) ? h->d_bscale : nullptr;
   p.minv = h->d_minv;
   p.acc = dacc;
+  p.nnzb = h->nnzb;
   double scale = 1.0, lam = 0.0;
   double acc[3];
   for (int it = 0; it < iters; ++it) {

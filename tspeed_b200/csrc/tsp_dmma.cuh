@@ -193,7 +193,8 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
       for (long long item = blockIdx.x + g * G; item < nitems && ok; item += NG * G) {
         const int e = int(item / ntile), tile = int(item % ntile);
         const int s0 = tile * ST, nsh = min(ST, S - s0);
-        const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+        int rb, nb;
+        row_span(p, e, rb, nb);
         const uint32_t bbytes = uint32_t(R) * KP * 8, xbytes = uint32_t(nsh) * R * 8;
         for (int b = 0; b < nb; ++b) {
           const int s = int(j % NSG);
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
             ok = false;
             break;
           }
-          const int c = p.col[rb + b];
+          const int c = col_at(p, rb + b);
           const uint32_t bar = smem_u32(&gfull[s]);
           const uint32_t dB = smem_u32(gst + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 8;
           fx_mbar_arrive_tx(bar, bbytes + xbytes);
@@ -249,7 +250,8 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
       if (int(it % NG) != grp) continue;  // another group's item (its own ring)
       const int e = int(item / ntile), tile = int(item % ntile);
       const int s0 = tile * ST;
-      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      int rb, nb;
+      row_span(p, e, rb, nb);
       // The epilogue's scalar inputs, requested now so that they arrive during
       // the products: the element's inverse-mass factor and, per m-tile,
       // whether the shot's source lies in this element.
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
 #pragma unroll
       for (int mt = 0; mt < MTW; ++mt) {
         const int sh = s0 + (wm * MTW + mt) * 8 + gs;
-        src_e[mt] = (sh < S) ? p.src_elem[sh] : -1;
+        src_e[mt] = (sh < S) ? src_elem_at(p, sh) : -1;
       }
       // u^{k-1} of this warp's outputs, requested now and used by the
       // epilogue: the loads overlap the products. u^k comes from the
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
           uk[mt][q] = make_double2(0.0, 0.0);
         }
       }
-      const bool diag_first = EPI == 1 && p.col[rb] == e;
+      const bool diag_first = EPI == 1 && col_at(p, rb) == e;
       double acc[MTW][NTW][2];
 #pragma unroll
       for (int mt = 0; mt < MTW; ++mt)
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
       }
       // ---- receivers (the condition is the same for every consumer warp) ----
       if (p.rcv_ptr != nullptr) {
-        const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+        const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
         if (q1 > q0) {
           // u^{k+1} of this item is visible to the whole group (barrier 1 + grp).
           asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(CF::NCW * 32) : "memory");
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
               const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
               const int sh = s0 + sl;
               if (sh >= S) continue;
-              const int rid = p.rcv_id[q];
+              const int rid = rcv_id_at(p, q);
               const double* ph = p.rcv_phi + size_t(rid) * NP;
               const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
               double v = 0.0;
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
               if (q >= npair) continue;
               const int sl = q / NP, r0 = 2 * (q - sl * NP);
               const int sh = s0 + sl;
-              const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+              const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
               const double u[2] = {uu[b].x, uu[b].y}, upr[2] = {up[b].x, up[b].y};
               double un[2];
 #pragma unroll
@@ -492,12 +494,12 @@ __global__ void __launch_bounds__(d64w_nt<R, NSG, NG, WM, WN, NU, RA>(), MINB)
         asm volatile("bar.sync %0, %1;" ::"r"(1 + ug), "n"(NUT) : "memory");
         if (!dead) {
           if (p.rcv_ptr != nullptr) {
-            const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+            const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
             const long long slot = k % p.seis_cap;
             for (int wk = ut; wk < (q1 - q0) * nsv * 2; wk += NUT) {
               const int cmp = wk & 1, sl = (wk >> 1) % nsv, q = q0 + (wk >> 1) / nsv;
               const int sh = s0 + sl;
-              const int rid = p.rcv_id[q];
+              const int rid = rcv_id_at(p, q);
               const double* ph = p.rcv_phi + size_t(rid) * NP;
               const double* un = p.out + base + size_t(sl) * R + cmp * NP;
               double v = 0.0;

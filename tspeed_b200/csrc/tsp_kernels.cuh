@@ -84,7 +84,61 @@ struct StepParams {
   // Non-finite watchdog (step modes only; null otherwise): set to 1 by any
   // kernel that writes a NaN or infinite u^{k+1}.
   int* nonfinite;
+  long long nnzb;             // blocks of the pattern (the checked build's row bounds)
 };
+
+// Gather indices of the step kernels -- row extents, neighbour ids, source
+// elements, receiver entries -- are read through these accessors. In the
+// checked build (TSP_CHECKED) each value is range-checked first: a value out
+// of range is recorded in g_index_check (site in the high word, the value in
+// the low word; the first failure of a launch sequence is kept) and replaced
+// by one inside the range, so the kernel reads only valid memory, completes,
+// and the host reports TSP_ERR_INDEX. Without TSP_CHECKED they are the plain
+// loads.
+enum IndexSite : int { kSiteRow = 1, kSiteCol = 2, kSiteSrcElem = 3, kSiteRcvPtr = 4, kSiteRcvId = 5, kSiteNeigh = 6 };
+#ifdef TSP_CHECKED
+__device__ unsigned long long g_index_check;
+__device__ __forceinline__ int checked_index(int v, int lo, int hi, int site) {
+  if (v >= lo && v < hi) return v;
+  atomicCAS(&g_index_check, 0ull, ((unsigned long long)(unsigned)site << 32) | (unsigned)v);
+  return lo;
+}
+#define TSP_INDEX(v, lo, hi, site) ::tsp::checked_index((v), (lo), (hi), (site))
+#else
+#define TSP_INDEX(v, lo, hi, site) (v)
+#endif
+
+// Block range [rb, rb + nb) of element row e: the diagonal block and at most
+// three neighbours inside the pattern (checked build: a row outside that is
+// recorded and clamped to a valid one).
+__device__ __forceinline__ void row_span(const StepParams& p, int e, int& rb, int& nb) {
+  rb = p.row_ptr[e];
+  nb = p.row_ptr[e + 1] - rb;
+#ifdef TSP_CHECKED
+  if (p.nnzb > 0 && (rb < 0 || rb >= p.nnzb || nb < 1 || nb > 4 || rb + nb > p.nnzb)) {
+    atomicCAS(&g_index_check, 0ull, ((unsigned long long)kSiteRow << 32) | (unsigned)e);
+    rb = min(max(rb, 0), int(p.nnzb - 1));
+    nb = min(max(nb, 1), min(4, int(p.nnzb - rb)));
+  }
+#endif
+}
+// Column (neighbour element) of block b of the pattern.
+template <class P>
+__device__ __forceinline__ int col_at(const P& p, long long b) {
+  return TSP_INDEX(p.col[b], 0, p.ne, kSiteCol);
+}
+// Source element of shot s (compared with element ids only; -1 for none).
+__device__ __forceinline__ int src_elem_at(const StepParams& p, int s) {
+  return TSP_INDEX(p.src_elem[s], -1, p.ne, kSiteSrcElem);
+}
+// Receiver entries of element e: [rcv_ptr[e], rcv_ptr[e + 1]) within the nrcv ids.
+__device__ __forceinline__ int rcv_ptr_at(const StepParams& p, int e) {
+  return TSP_INDEX(p.rcv_ptr[e], 0, p.nrcv + 1, kSiteRcvPtr);
+}
+// Receiver id of entry q (indexes rcv_phi and the seismogram buffer).
+__device__ __forceinline__ int rcv_id_at(const StepParams& p, int q) {
+  return TSP_INDEX(p.rcv_id[q], 0, p.nrcv, kSiteRcvId);
+}
 
 // Raises the non-finite flag when a new displacement pair holds a NaN or an
 // infinity (the leap-frog recurrence keeps such a value for good).
@@ -181,11 +235,10 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
   int rb = 0, nb = 0;
   double (*xt)[R] = xs[warp][tw < TPW ? tw : 0];
   if (active) {
-    rb = p.row_ptr[e];
-    nb = p.row_ptr[e + 1] - rb;
+    row_span(p, e, rb, nb);
     // Gather x of the row's block columns: contiguous 2Np modes per element.
     for (int b = 0; b < nb; ++b) {
-      const int c = p.col[rb + b];
+      const int c = col_at(p, rb + b);
       const double2* src = reinterpret_cast<const double2*>(p.x + (size_t(c) * S + sh) * R);
       const double xs = (p.mode == kModePower) ? (p.xscale_mesh ? p.xscale_mesh[p.mesh_of[e]] : p.xscale) : 1.0;
       for (int q = tl; q < NPAIR; q += T) {
@@ -251,7 +304,7 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
     const double mi = p.minv[e];
     // Source row: the shot's own source (one per shot), or in a multi-mesh
     // group the source of this element's mesh.
-    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && p.src_elem[sh] == e) ? sh : -1);
+    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && src_elem_at(p, sh) == e) ? sh : -1);
     const bool is_src = (srow >= 0) && (k < p.nF) && (p.mode == kModeStep || p.mode == kModeFirst);
     double Fk[2] = {0.0, 0.0};
     if (is_src) {
@@ -318,8 +371,8 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
     __syncwarp();
     int r0 = 0, r1 = 0;
     if (active) {
-      r0 = p.rcv_ptr[e];
-      r1 = p.rcv_ptr[e + 1];
+      r0 = rcv_ptr_at(p, e);
+      r1 = rcv_ptr_at(p, e + 1);
       if (r1 > r0) {
 #pragma unroll
         for (int s = 0; s < PPL; ++s) {
@@ -335,7 +388,7 @@ __global__ void __launch_bounds__(256) k_step_rows(const StepParams p) {
     if (active && r1 > r0) {
       const long long slot = k % p.seis_cap;
       for (int t = tl; t < 2 * (r1 - r0); t += T) {
-        const int rid = p.rcv_id[r0 + t / 2];
+        const int rid = rcv_id_at(p, r0 + t / 2);
         const int comp = t & 1;
         const double* ph = p.rcv_phi + size_t(rid) * NP;
         double v = 0.0;
@@ -451,8 +504,8 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
   const int t = threadIdx.x;
   const int tx = t & 15, ty = t >> 4;
   const bool comp = ty < CF::TY;
-  const int rb = p.row_ptr[e];
-  const int nb = p.row_ptr[e + 1] - rb;
+  int rb, nb;
+  row_span(p, e, rb, nb);
   const BT* blocks = reinterpret_cast<const BT*>(p.blocks);
 
   AT acc[4][4];
@@ -462,7 +515,7 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
     for (int j = 0; j < 4; ++j) acc[i][j] = AT(0);
 
   for (int b = 0; b < nb; ++b) {
-    const int c = p.col[rb + b];
+    const int c = col_at(p, rb + b);
     // Stage the block (already in the padded column-major layout).
     const BT* gb = blocks + size_t(rb + b) * R * RP;
     for (int i = t; i < R * RP; i += CF::NT) Bs[i] = to_acc<BT, AT>(gb[i]);
@@ -504,7 +557,7 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
       const int sh = s0 + 4 * tx + i;
       if (sh >= S) continue;
       const size_t me = (size_t(e) * S + sh) * R;
-      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
       double Fk[2] = {0.0, 0.0};
       if (is_src) {
         Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
@@ -540,7 +593,7 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
 
   // ---- receivers ----
   if (p.rcv_ptr != nullptr) {
-    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
     if (q1 > q0) {
       __syncthreads();  // this CTA's writes of u^{k+1} are visible after the barrier
       const long long slot = k % p.seis_cap;
@@ -549,7 +602,7 @@ __global__ void __launch_bounds__(BatchCfg<R>::NT) k_step_batched(const StepPara
         const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
         const int sh = s0 + sl;
         if (sh >= S) continue;
-        const int rid = p.rcv_id[q];
+        const int rid = rcv_id_at(p, q);
         const double* ph = p.rcv_phi + size_t(rid) * NP;
         const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
         double v = 0.0;
@@ -652,8 +705,8 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int wm = w % CF::WM, wn = w / CF::WM;
   const int g = lane >> 2, tg = lane & 3;
-  const int rb = p.row_ptr[e];
-  const int nb = p.row_ptr[e + 1] - rb;
+  int rb, nb;
+  row_span(p, e, rb, nb);
   const double* blocks = reinterpret_cast<const double*>(p.blocks);
   const int nsh = min(ST, S - s0);  // shots of this tile
 
@@ -683,7 +736,7 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
       const int k = i / NP, j = i - k * NP;
       cp_async16(B + k * PS + 2 * j, gb + size_t(k) * p.bpitch + 2 * j);
     }
-    const int c = p.col[rb + b];
+    const int c = col_at(p, rb + b);
     const double* gx = p.x + (size_t(c) * S + s0) * R;
     for (int i = t; i < nsh * NP; i += CF::NT) {
       const int r = i / NP, j = i - r * NP;
@@ -738,7 +791,7 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
     const int sh = s0 + (wm * MTW + mt) * 8 + g;
     if (sh >= S) continue;
     const size_t me = (size_t(e) * S + sh) * R;
-    const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+    const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
     double Fk[2] = {0.0, 0.0};
     if (is_src) {
       Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
@@ -772,7 +825,7 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
 
   // ---- receivers ----
   if (p.rcv_ptr != nullptr) {
-    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
     if (q1 > q0) {
       __syncthreads();  // this CTA's writes of u^{k+1} are visible after the barrier
       const long long slot = k % p.seis_cap;
@@ -781,7 +834,7 @@ __global__ void __launch_bounds__(D64Cfg<R>::NT, 3) k_step_batched64d(const Step
         const int cmp = wk & 1, sl = (wk >> 1) % ST, q = q0 + (wk >> 1) / ST;
         const int sh = s0 + sl;
         if (sh >= S) continue;
-        const int rid = p.rcv_id[q];
+        const int rid = rcv_id_at(p, q);
         const double* ph = p.rcv_phi + size_t(rid) * NP;
         const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
         double v = 0.0;
@@ -841,8 +894,8 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
   const int t = threadIdx.x;
   const int tx = t & 15, ty = t >> 4;
   const bool comp = ty < CF::TY;
-  const int rb = p.row_ptr[e];
-  const int nb = p.row_ptr[e + 1] - rb;
+  int rb, nb;
+  row_span(p, e, rb, nb);
 
   // ---- stage every block of the row and every neighbour tile ----
   {
@@ -850,7 +903,7 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
     const int nbc = nb * R * RP / 4;  // 16-byte chunks, blocks contiguous in HBM
     for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
     for (int b = 0; b < nb; ++b) {
-      const int c = p.col[rb + b];
+      const int c = col_at(p, rb + b);
       const float* gx = p.x32_in + (size_t(c) * ntile + tile) * R * ST;
       float* sx = Xs + b * R * SP;
       for (int i = t; i < R * (ST / 4); i += CF::NT) {
@@ -900,7 +953,7 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
       const int sh = s0 + 4 * tx + i;
       if (sh >= S) continue;
       const size_t me = (size_t(e) * S + sh) * R;
-      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
       double Fk[2] = {0.0, 0.0};
       if (is_src) {
         Fk[0] = p.F[(size_t(sh) * p.nF + k) * 2];
@@ -942,7 +995,7 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
 
   // ---- receivers ----
   if (p.rcv_ptr != nullptr) {
-    const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+    const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
     if (q1 > q0) {
       __syncthreads();
       const long long slot = k % p.seis_cap;
@@ -951,7 +1004,7 @@ __global__ void __launch_bounds__(Batch32Cfg<R>::NT) k_step_batched32(const Step
         const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
         const int sh = s0 + sl;
         if (sh >= S) continue;
-        const int rid = p.rcv_id[q];
+        const int rid = rcv_id_at(p, q);
         const double* ph = p.rcv_phi + size_t(rid) * NP;
         const double* un = p.out + (size_t(e) * S + sh) * R + cmp * NP;
         double v = 0.0;
@@ -1073,7 +1126,8 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
   auto issue_operands = [&](long long item, float* st) {
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
-    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    int rb, nb;
+    row_span(p, e, rb, nb);
     float* Bs = st;
     float* Xs = st + 4 * R * RP;
     const float* gb = reinterpret_cast<const float*>(p.blocks) + size_t(rb) * R * RP;
@@ -1081,7 +1135,7 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
     for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
     const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
     for (int b = 0; b < nb; ++b) {
-      const int c = p.col[rb + b];
+      const int c = col_at(p, rb + b);
       const float* gx = p.x32_in + (size_t(c) * nsh_tile + sht) * R * NTILE_SH + sho;
       float* sx = Xs + b * R * ST;
       for (int i = t; i < R * (ST / 4); i += CF::NT) {
@@ -1112,7 +1166,8 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
     const int nsv = min(ST, S - s0);
-    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    int rb, nb;
+    row_span(p, e, rb, nb);
     float* st = stage0 + buf * CF::STAGE;
     issue_state(item);
     asm volatile("cp.async.commit_group;\n" ::: "memory");  // T_i
@@ -1147,7 +1202,7 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
     for (int w = t; w < nsv * NPAIR; w += CF::NT) {
       const int sl = w / NPAIR, q = w - sl * NPAIR;
       const int sh = s0 + sl, r0 = 2 * q;
-      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
       const double2 uu = *reinterpret_cast<const double2*>(Uk + sl * UP + r0);
       const double2 up = p.uprev ? *reinterpret_cast<const double2*>(Up + sl * UP + r0) : make_double2(0.0, 0.0);
       const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
@@ -1189,14 +1244,14 @@ __global__ void __launch_bounds__(PipeCfg<R, ST, TR>::NT, 1) k_step_batched32p(c
     }
 
     if (p.rcv_ptr != nullptr) {
-      const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+      const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
       if (q1 > q0) {
         const long long slot = k % p.seis_cap;
         const int nwork = (q1 - q0) * ST * 2;
         for (int w = t; w < nwork; w += CF::NT) {
           const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
           if (sl >= nsv) continue;
-          const int rid = p.rcv_id[q];
+          const int rid = rcv_id_at(p, q);
           const double* ph = p.rcv_phi + size_t(rid) * NP;
           // u^{k+1} of this item was written to global by the whole CTA
           // before the barrier above.
@@ -1275,7 +1330,8 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
   auto issue_operands = [&](long long item, float* st) {
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
-    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    int rb, nb;
+    row_span(p, e, rb, nb);
     float* Bs = st;
     float* Xs = st + 4 * R * RP;
     const float* gb = reinterpret_cast<const float*>(p.blocks) + size_t(rb) * R * RP;
@@ -1283,7 +1339,7 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
     for (int i = t; i < nbc; i += CF::NT) cp_async16(Bs + 4 * i, gb + 4 * i);
     const int sht = s0 / NTILE_SH, sho = s0 - sht * NTILE_SH;
     for (int b = 0; b < nb; ++b) {
-      const int c = p.col[rb + b];
+      const int c = col_at(p, rb + b);
       const float* gx = p.x32_in + (size_t(c) * nsh_tile + sht) * R * NTILE_SH + sho;
       float* sx = Xs + b * R * ST;
       for (int i = t; i < R * (ST / 4); i += CF::NT) {
@@ -1302,7 +1358,8 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
     const int e = int(item / ntile), tile = int(item - (long long)e * ntile);
     const int s0 = tile * ST;
     const int nsv = min(ST, S - s0);
-    const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+    int rb, nb;
+    row_span(p, e, rb, nb);
     float* st = stage0 + buf * CF::STAGE;
     const long long nxt = item + gridDim.x;
     if (nxt < nitems) issue_operands(nxt, stage0 + (buf ^ 1) * CF::STAGE);
@@ -1333,7 +1390,7 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
       const int sl = w / NPAIR, q = w - sl * NPAIR;
       const int sh = s0 + sl, r0 = 2 * q;
       const size_t me = (size_t(e) * S + sh) * R + r0;
-      const bool is_src = (p.src_elem[sh] == e) && (k < p.nF);
+      const bool is_src = (src_elem_at(p, sh) == e) && (k < p.nF);
       const double2 uu = __ldg(reinterpret_cast<const double2*>(p.x + me));
       const double2 up = p.uprev ? *reinterpret_cast<const double2*>(p.uprev + me) : make_double2(0.0, 0.0);
       const double u[2] = {uu.x, uu.y}, upv[2] = {up.x, up.y};
@@ -1375,14 +1432,14 @@ __global__ void __launch_bounds__(KsplitCfg<R>::NT, 1) k_step_batched32k(const S
       }
     }
     if (p.rcv_ptr != nullptr) {
-      const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+      const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
       if (q1 > q0) {
         const long long slot = k % p.seis_cap;
         const int nwork = (q1 - q0) * ST * 2;
         for (int w = t; w < nwork; w += CF::NT) {
           const int cmp = w & 1, sl = (w >> 1) % ST, q = q0 + (w >> 1) / ST;
           if (sl >= nsv) continue;
-          const int rid = p.rcv_id[q];
+          const int rid = rcv_id_at(p, q);
           const double* ph = p.rcv_phi + size_t(rid) * NP;
           const double* un = p.out + (size_t(e) * S + s0 + sl) * R + cmp * NP;
           double v = 0.0;
@@ -1591,9 +1648,9 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
     // ---- faces ----
 #pragma unroll 1
     for (int l = 0; l < 3; ++l) {
-      const int nb = q.neigh[3 * size_t(e) + l];
+      const int nb = TSP_INDEX(q.neigh[3 * size_t(e) + l], -1, p.ne, kSiteNeigh);
       if (nb < 0) continue;
-      const int lp = q.nedge[3 * size_t(e) + l];
+      const int lp = TSP_INDEX(q.nedge[3 * size_t(e) + l], 0, 3, kSiteNeigh);
       const double* xgn = p.x + size_t(nb) * R;
       for (int t = lane; t < R; t += 32) {
         double v = __ldg(xgn + t);
@@ -1675,7 +1732,7 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
     }
     // ---- epilogue (rows i: component 0 at i, component 1 at NP + i) ----
     const double mi = p.minv[e];
-    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && p.src_elem[0] == e) ? 0 : -1);
+    const int srow = p.src_of ? p.src_of[e] : ((p.src_elem != nullptr && src_elem_at(p, 0) == e) ? 0 : -1);
     const bool is_src = (srow >= 0) && (k < p.nF) && (p.mode == kModeStep || p.mode == kModeFirst);
     const double dt = p.dt_elem ? p.dt_elem[e] : p.dt;
     double* og = p.out + size_t(e) * R;
@@ -1728,12 +1785,12 @@ __global__ void __launch_bounds__(MFCfg<N>::WARPS * 32) k_step_matfree(const Ste
     }
     // receivers of this element
     if (p.rcv_ptr != nullptr && (p.mode == kModeStep || p.mode == kModeFirst)) {
-      const int r0 = p.rcv_ptr[e], r1 = p.rcv_ptr[e + 1];
+      const int r0 = rcv_ptr_at(p, e), r1 = rcv_ptr_at(p, e + 1);
       if (r1 > r0) {
         __syncwarp();  // og written by the whole warp
         const long long slot = k % p.seis_cap;
         for (int t = lane; t < 2 * (r1 - r0); t += 32) {
-          const int rid = p.rcv_id[r0 + t / 2], c = t & 1;
+          const int rid = rcv_id_at(p, r0 + t / 2), c = t & 1;
           const double* ph = p.rcv_phi + size_t(rid) * NP;
           double v = 0.0;
           for (int i = 0; i < NP; ++i) v += ph[i] * og[c * NP + i];
@@ -1906,13 +1963,13 @@ __global__ void __launch_bounds__(256) k_assemble(const AssembleParams p) {
     }
   } else if (t <= 7 && t - 4 < nb) {
     const int q = t - 4, face = p.bface[rb + q];
-    if (face >= 0) face_beta(p, p.col[rb + q], p.nedge[3 * size_t(e) + face], betan[q]);
+    if (face >= 0) face_beta(p, col_at(p, rb + q), p.nedge[3 * size_t(e) + face], betan[q]);
   }
   __syncthreads();
   const int R = 2 * p.Np;
   const int RR = R * R;
   for (int q = 0; q < nb; ++q) {
-    const int b = rb + q, c = p.col[b], face = p.bface[b];
+    const int b = rb + q, c = col_at(p, b), face = p.bface[b];
     float inv_sc = 1.0f;
     if (p.prec == 2) {
       float amax = 0.0f;

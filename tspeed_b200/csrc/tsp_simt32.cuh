@@ -121,8 +121,8 @@ __device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, fl
 __device__ __forceinline__ unsigned long long tile_source_mask(const StepParams& p, int e, int s0, int nsv,
                                                                long long k, int ln) {
   if (k >= p.nF) return 0ull;
-  const bool a = ln < nsv && p.src_elem[s0 + ln] == e;
-  const bool b = ln + 32 < nsv && p.src_elem[s0 + 32 + ln] == e;
+  const bool a = ln < nsv && src_elem_at(p, s0 + ln) == e;
+  const bool b = ln + 32 < nsv && src_elem_at(p, s0 + 32 + ln) == e;
   return (unsigned long long)__ballot_sync(0xffffffffu, a) | ((unsigned long long)__ballot_sync(0xffffffffu, b) << 32);
 }
 
@@ -251,7 +251,8 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
       bool ok = true;
       for (long long item = blockIdx.x + g * G; item < nitems && ok; item += NGR * G) {
         const int e = int(item / ntile), tile = int(item % ntile);
-        const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+        int rb, nb;
+        row_span(p, e, rb, nb);
         for (int b = 0; b < nb; ++b) {
           const int s = int(j % NSG);
           const uint32_t n = j / NSG;
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
             ok = false;
             break;
           }
-          const int c = p.col[rb + b];
+          const int c = col_at(p, rb + b);
           const uint32_t bar = smem_u32(&gfull[s]);
           const uint32_t dB = smem_u32(gst + size_t(s) * CF::STAGE), dX = dB + CF::BSZ * 4;
           fx_mbar_arrive_tx(bar, bbytes + xbytes);
@@ -294,7 +295,8 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
     for (long long item = blockIdx.x; item < nitems; item += G, ++it) {
       if (int(it % NGR) != grp) continue;  // another pair's item
       const int e = int(item / ntile);
-      const int rb = p.row_ptr[e], nb = p.row_ptr[e + 1] - rb;
+      int rb, nb;
+      row_span(p, e, rb, nb);
       float acc[RL][8];
       unsigned long long acc2[RL][4];  // F2: shots (2m, 2m + 1) of the lane's 8
 #pragma unroll
@@ -415,12 +417,12 @@ __global__ void __launch_bounds__(S32WLayout<R, NGR, NSG, NU>::NT, 1)
         }
         // Receivers of this element.
         if (p.rcv_ptr != nullptr) {
-          const int q0 = p.rcv_ptr[e], q1 = p.rcv_ptr[e + 1];
+          const int q0 = rcv_ptr_at(p, e), q1 = rcv_ptr_at(p, e + 1);
           const long long slot = k % p.seis_cap;
           for (int wk = ut; wk < (q1 - q0) * nsv * 2; wk += NUT) {
             const int cmp = wk & 1, sl = (wk >> 1) % nsv, q = q0 + (wk >> 1) / nsv;
             const int sh = s0 + sl;
-            const int rid = p.rcv_id[q];
+            const int rid = rcv_id_at(p, q);
             const double* ph = p.rcv_phi + size_t(rid) * NP;
             const double* un = p.out + base + size_t(sl) * R + cmp * NP;
             double v = 0.0;

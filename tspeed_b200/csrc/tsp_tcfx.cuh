@@ -268,10 +268,9 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
       int rb = 0, nb = 0, cols[4] = {0, 0, 0, 0};
       if (item < nitems) {
         const int e0 = int(item / ntile);
-        rb = p.row_ptr[e0];
-        nb = p.row_ptr[e0 + 1] - rb;
+        row_span(p, e0, rb, nb);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) cols[b] = b < nb ? p.col[rb + b] : 0;
+        for (int b = 0; b < 4; ++b) cols[b] = b < nb ? col_at(p, rb + b) : 0;
       }
       bool ok = true;
       for (; item < nitems && ok; item += G) {
@@ -280,8 +279,7 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
         int rbn = 0, nbn = 0, coln[4] = {0, 0, 0, 0};
         if (nxt < nitems) {
           const int en = int(nxt / ntile);
-          rbn = p.row_ptr[en];
-          nbn = p.row_ptr[en + 1] - rbn;
+          row_span(p, en, rbn, nbn);
         }
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
@@ -305,7 +303,7 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
           ++j;
           if (b == 0 && nxt < nitems) {
 #pragma unroll
-            for (int bb = 0; bb < 4; ++bb) coln[bb] = bb < nbn ? p.col[rbn + bb] : 0;
+            for (int bb = 0; bb < 4; ++bb) coln[bb] = bb < nbn ? col_at(p, rbn + bb) : 0;
           }
         }
         rb = rbn;
@@ -346,7 +344,8 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
       int nb = 0;
       if (item < nitems) {
         const int e0 = int(item / ntile);
-        nb = p.row_ptr[e0 + 1] - p.row_ptr[e0];
+        int rb0;
+        row_span(p, e0, rb0, nb);
       }
       bool ok = true;
       for (; item < nitems && ok; item += G) {
@@ -354,8 +353,9 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
         int rp0 = 0, rp1 = 0;
         if (nxt < nitems) {
           const int en = int(nxt / ntile);
-          rp0 = p.row_ptr[en];
-          rp1 = p.row_ptr[en + 1];
+          int nbx;
+          row_span(p, en, rp0, nbx);
+          rp1 = rp0 + nbx;
         }
         for (int b = 0; b < nb; ++b, ++j) {
           const int s = int(j % NST), a = int(j % NACC);
@@ -413,8 +413,9 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
     int rp0 = 0, rp1 = 0;
     if (item < nitems) {
       const int e0 = int(item / ntile);
-      rp0 = p.row_ptr[e0];
-      rp1 = p.row_ptr[e0 + 1];
+      int nbx;
+      row_span(p, e0, rp0, nbx);
+      rp1 = rp0 + nbx;
     }
     bool ok = true;
     for (; item < nitems && ok; item += G, ++li) {
@@ -422,8 +423,9 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
       const long long nxt = item + G;
       if (nxt < nitems) {
         const int en = int(nxt / ntile);
-        rp0 = p.row_ptr[en];
-        rp1 = p.row_ptr[en + 1];
+        int nbx;
+        row_span(p, en, rp0, nbx);
+        rp1 = rp0 + nbx;
       }
       // yacc[4 i + 2 v + h]: shot (v ? shb : sha), row 8(ch0 + i) + rc + h;
       // the row's blocks accumulate in registers, in FP64, in block order.
@@ -530,10 +532,10 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
       const int s02 = t2 * M, nsv2 = min(M, S - s02);
       mi_n = p.minv[e2];
       if (p.rcv_ptr != nullptr) {
-        q0_n = p.rcv_ptr[e2];
-        q1_n = p.rcv_ptr[e2 + 1];
+        q0_n = rcv_ptr_at(p, e2);
+        q1_n = rcv_ptr_at(p, e2 + 1);
       }
-      src_n = (ut < nsv2) ? p.src_elem[s02 + ut] : -1;
+      src_n = (ut < nsv2) ? src_elem_at(p, s02 + ut) : -1;
     };
     // A warp that gives up (timeout or another role's abort) keeps walking
     // the item loop without work so that every named barrier below is still
@@ -640,7 +642,7 @@ __global__ void __launch_bounds__(FxCfg<R>::NT, 1) k_step_batched_fx(const StepP
         for (int w = ut; w < nwork; w += NUPT) {
           const int cmp = w & 1, s2 = (w >> 1) % M, q = q0 + (w >> 1) / M;
           if (s2 >= nsv) continue;
-          const int rid = p.rcv_id[q];
+          const int rid = rcv_id_at(p, q);
           const double* ph = p.rcv_phi + size_t(rid) * NP;
           const double* un = Ys + s2 * YS + cmp * NP;
           double v = 0.0;
