@@ -615,6 +615,17 @@ def main():
         line["plain_fp64_single_shot"] = {"value": v1, "unit": UNIT, "ms_per_step": ms1 / K,
                                           "roofline_frac": a1 / hbm, "achieved_gbs": a1}
         line["speedup_vs_plain_fp64"] = value / v1
+        # The FP32-operator single-shot drop-in on the same mesh and shot.
+        with capi.Simulation.from_problem(p1, precision="fp32") as s1f:
+            prepare(s1f, p1, dt, K + Wm + 2)
+            s1f.first_step()
+            s1f.run(Wm)
+            s1f.run_timed(K)
+            ms1f = s1f.run_timed(K)
+        a1f = bytes_per_step(p1.mesh.ne, p1.Np, nnzb1, 1, "fp32") / (ms1f / K / 1e3) / 1e9
+        line["plain_fp32_operator_single_shot"] = {"value": p1.dofs_per_shot * K / (ms1f / 1e3), "unit": UNIT,
+                                                   "ms_per_step": ms1f / K, "roofline_frac": a1f / hbm,
+                                                   "achieved_gbs": a1f, "speedup_vs_plain_fp64": ms1 / ms1f}
         # Mixed precision for all shots: FP32 operator, autotuned batched kernel.
         if prob.nshots > 1 and args.precision == "fp64":
             with capi.Simulation.from_problem(prob, precision="fp32") as s32:
