@@ -213,15 +213,20 @@ struct RowTeam {
 
 // Columns per unrolled step of k_step_rows' block loop: enough block loads in
 // flight per lane to stream the blocks at the HBM rate. FP64 blocks: 8
-// columns (8 x 16 bytes per lane); 4- and 2-byte blocks: the largest divisor
-// of 2Np up to 32 (28 at 2Np = 56, 21 at 42). Measured on 160,000 triangles,
-// N = 6, one shot, FP32 blocks: 8 columns 1.629 ms per step (78 % of the
-// measured HBM bandwidth), 14 columns 1.362 ms (94 %), 28 columns 1.237 ms
-// (103 %). The FMA chains keep their column order: the same bits either way.
+// columns where 2Np is a multiple of 8, else the largest divisor of 2Np up to
+// 21; 4- and 2-byte blocks: the largest divisor of 2Np up to 32 (28 at
+// 2Np = 56, 21 at 42). Measured, one shot (fractions of the measured HBM
+// copy bandwidth): 160,000 triangles, N = 6, FP32 blocks, 8 columns 1.629 ms
+// per step (78 %), 14 columns 1.362 ms (94 %), 28 columns 1.237 ms (103 %);
+// FP64 blocks 8 columns 2.394 ms (105 %), 14 columns 2.415 ms; 40,000
+// triangles, N = 5, FP64 blocks, 8 columns 0.386 ms (92 %), 14 columns
+// 0.351 ms (101 %), 21 columns 0.349 ms (102 %). The FMA chains keep their
+// column order: the same bits either way.
 template <int R, typename BT>
 constexpr int row_unroll() {
-  if (sizeof(BT) == 8) return 8;
-  int u = R < 32 ? R : 32;
+  if (sizeof(BT) == 8 && R % 8 == 0) return 8;
+  const int cap = sizeof(BT) == 8 ? 21 : 32;
+  int u = R < cap ? R : cap;
   while (R % u != 0) --u;
   return u;
 }
