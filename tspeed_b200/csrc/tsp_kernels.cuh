@@ -222,10 +222,14 @@ struct RowTeam {
 // triangles, N = 5, FP64 blocks, 8 columns 0.386 ms (92 %), 14 columns
 // 0.351 ms (101 %), 21 columns 0.349 ms (102 %). The FMA chains keep their
 // column order: the same bits either way.
+// Lanes that own two row pairs (2Np > 64) hold twice the loads per column:
+// the cap is halved there, which keeps 2Np = 72 at two CTAs per SM (FP32
+// blocks unrolled by 24 took 136 registers, one CTA).
 template <int R, typename BT>
 constexpr int row_unroll() {
   if (sizeof(BT) == 8 && R % 8 == 0) return 8;
-  const int cap = sizeof(BT) == 8 ? 21 : 32;
+  const int ppl = (R / 2 + 31) / 32;
+  const int cap = (sizeof(BT) == 8 ? 21 : 32) / ppl;
   int u = R < cap ? R : cap;
   while (R % u != 0) --u;
   return u;
